@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""k-mers queried per second on B200 GPUs (one process per GPU).
+
+Default workload (the large configuration): a seeded 100 Mbp genome (41% GC,
+i.i.d.) plus 5% of its length as inserted 1-10 kbp repeat copies mutated at
+0.1%; SBWT of all its 31-mers; presearch depth p = 12; 10M reads of 150 bp
+(10% genome-sampled with 1% substitutions, 90% uniform random) = 1.2G k-mers.
+
+One step = one pass of the search path over the whole batch:
+  `value`: letters + row table resident in HBM -> pack -> per-row k-mer table
+           -> persistent search kernel -> u64 answers + membership bitmap,
+           timed with CUDA events on the launching stream (inputs and outputs,
+           1.5 GB + 9.6 GB, are larger than L2; no flush needed);
+  `e2e`:   the same through sbwt_search_reads_host with pinned host buffers:
+           letters and row starts host->device, answers device->host, inside
+           the timed region (host wall clock around the synchronous call).
+With --gpus N (torchrun), every rank holds a replica of the index and searches
+its own 10M reads (weak scaling, no collective on the data path); the time
+is the max over ranks.
+
+--impl reference times the reference's search semantics on the host cores:
+the reference has no CPU search, so its arm is the C restatement in oracle/
+(OpenMP, all host threads), on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+METRIC = "k-mers queried/sec on 1 B200, plain vs learned-prefiltered search, bit-exact"
+UNIT = "k-mers/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scale", type=float, default=1.0, help="shrinks the workload (tests only)")
+    ap.add_argument("--p", type=int, default=12)
+    ap.add_argument("--kpt", type=int, default=0)
+    ap.add_argument("--tpk", type=int, default=0)
+    ap.add_argument("--tpb", type=int, default=0)
+    ap.add_argument("--layout", choices=["lines", "poppy"], default="lines")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload(scale, rank):
+    from sbwt_gpu_b200 import workloads as wl
+    rng = wl.rng_for(1236)
+    n = int(100_000_000 * scale)
+    genome = wl.random_bases(rng, n, gc=0.41)
+    genome = wl.with_repeats(rng, genome, int(0.05 * n))
+    rrng = wl.rng_for(7000 + rank)
+    n_reads = max(10, int(10_000_000 * scale))
+    n_pos = n_reads // 10
+    letters, rows = wl.mixed_reads(rrng, genome, n_pos, n_reads - n_pos, 150, 0.01)
+    return genome, letters, rows
+
+
+def measured_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                smax.append(float(f[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference(ox, letters, rows, k, p, budget_s, table):
+    """The oracle port on a bounded prefix of the reads: (k-mers/s, answers, steps, rows used)."""
+    import oracle as orc
+    threads = orc.num_threads()
+    # calibrate on a small prefix, then size the sample to the budget
+    r0 = min(rows.size - 1, 2000)
+    t = time.perf_counter()
+    ox.search_reads(letters[: int(rows[r0])], rows[: r0 + 1], k, p, table)
+    rate = (r0 * 120) / max(time.perf_counter() - t, 1e-6)
+    want_kmers = rate * budget_s
+    nr = int(min(rows.size - 1, max(r0, want_kmers / 120)))
+    sub_rows = rows[: nr + 1]
+    sub_letters = letters[: int(sub_rows[-1])]
+    t = time.perf_counter()
+    ans, steps = ox.search_reads(sub_letters, sub_rows, k, p, table, want_steps=True)
+    dt = time.perf_counter() - t
+    return ans.size / dt, ans, steps, nr, threads
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    k = 31
+    p = args.p
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        return reference_arm(args, k, p)
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+
+    import sbwt_gpu_b200 as sg
+    import oracle as orc
+
+    genome, letters, rows = workload(args.scale, rank)
+    n_kmers = sg.count_kmers(rows, k)
+    # the index: rank 0 builds the SBWT and writes the reference's files; every rank loads them
+    tmpdir = os.environ.get("SBWT_BENCH_DIR") or os.path.join(tempfile.gettempdir(), f"sbwt_bench_{os.getppid()}")
+    os.makedirs(tmpdir, exist_ok=True)
+    prefix = os.path.join(tmpdir, "ix")
+    if rank == 0:
+        t = time.perf_counter()
+        built = sg.build_sbwt([genome.tobytes()], k)
+        build_s = time.perf_counter() - t
+        paths = sg.write_index_files(prefix, built)
+        n_columns = built.n_bits
+        del built
+    if world > 1:
+        dist.barrier()
+    paths = [f"{prefix}.{c}" for c in "ACGT"]
+    layout = sg.SBWT_LAYOUT_POPPY if args.layout == "poppy" else sg.SBWT_LAYOUT_LINES
+    t = time.perf_counter()
+    ix = sg.Index.load(*paths, k=k, k_presearch=p, device=local_rank, layout=layout,
+                       kmers_per_thread=args.kpt, threads_per_kmer=args.tpk, threads_per_block=args.tpb)
+    load_s = time.perf_counter() - t
+    info = ix.info()
+
+    d_letters = torch.from_numpy(letters).to(dev)
+    d_rows = torch.from_numpy(rows.view(np.int64)).to(dev)
+    d_ans = torch.empty(n_kmers, dtype=torch.int64, device=dev)
+    d_mem = torch.empty((n_kmers + 31) // 32, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    ix.profile(True)
+
+    def step():
+        ix.search_reads(d_letters, d_rows, d_ans, n_kmers, d_member_bits=d_mem, stream=stream)
+
+    for _ in range(max(args.warmup, 0)):
+        step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clocks = Clocks(local_rank)
+    clocks.start()
+    torch.cuda.synchronize(dev)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    search_ms, launches = [], 0
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+        prof = ix.last_profile()  # CUDA events of this step's kernels (on `stream`)
+        search_ms.append(prof["search_ms"])
+        launches += prof["launches"]
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    total_ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    if world > 1:
+        dist.barrier()
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = n_kmers * world * args.steps / (total_ms / 1e3)
+
+    # ---- correctness on a sample + the CPU baseline (rank 0 only, untimed)
+    cpu = None
+    mean_steps = None
+    if rank == 0:
+        ox = orc.OracleIndex.from_files(paths)
+        table = ox.presearch(p) if p else None
+        rate, ans, steps, nr, threads = cpu_reference(ox, letters, rows, k, p, args.cpu_seconds, table)
+        got = d_ans[: ans.size].cpu().numpy().view(np.uint64)
+        if not np.array_equal(got, ans):
+            raise SystemExit(f"bench: {int((got != ans).sum())} of {ans.size} sampled answers differ from the oracle")
+        mean_steps = float(steps.mean())
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"first {nr} reads ({ans.size} k-mers) of the same batch, C restatement of the reference "
+                         f"search (the reference has no CPU search), OpenMP schedule(dynamic,4096)"}
+
+    # ---- end to end through the host entry point (pinned buffers)
+    e2e = None
+    if not args.no_e2e:
+        h_letters = torch.from_numpy(letters).pin_memory()
+        h_rows = torch.from_numpy(rows.view(np.int64)).pin_memory()
+        h_ans = torch.empty(n_kmers, dtype=torch.int64).pin_memory()
+        ix.profile(False)
+        ix.search_reads_host(h_letters, h_rows, h_ans)  # warm-up
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        t = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            ix.search_reads_host(h_letters, h_rows, h_ans)
+        e2e_s = time.perf_counter() - t
+        if world > 1:
+            tt = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e2e_s = float(tt.item())
+        if rank == 0 and not np.array_equal(h_ans[: ans.size].numpy().view(np.uint64), ans):
+            raise SystemExit("bench: end-to-end answers differ from the oracle")
+        e2e = {"value": n_kmers * world * args.e2e_steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(letters.nbytes + rows.nbytes), "d2h_bytes_per_step": int(n_kmers * 8)}
+
+    if rank == 0:
+        peak, peak_kind = measured_hbm()
+        kern_ms = statistics.mean(search_ms)
+        q = (letters.size / 4.0) / n_kmers
+        b_kmer = 128.0 * mean_steps + 16 + 8 + q
+        achieved = n_kmers * b_kmer / (kern_ms / 1e3) / 1e9
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "search_kernel_traffic.json")
+        if os.path.exists(tp):
+            try:
+                traffic = float(json.load(open(tp))["dram_bytes_per_kmer"]) * n_kmers
+            except Exception:
+                traffic = None
+        hits = int((d_ans.cpu().numpy().view(np.uint64) != orc.NOT_FOUND).sum())
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded)",
+            "config": {
+                "workload": "large: 100 Mbp genome (41% GC) + 5% repeats, SBWT k=31, p=12, "
+                            "10M reads x 150 bp (10% genome-sampled with 1% subs, 90% random)"
+                if args.scale == 1.0 else f"large x{args.scale}",
+                "n_kmers_per_gpu": n_kmers, "n_columns": info["n_bits"], "k": k, "p": p,
+                "layout": args.layout, "present_kmers": hits,
+                "l2": "inputs and outputs larger than L2 (letters %.2f GB, answers %.2f GB); no flush" % (
+                    letters.nbytes / 1e9, n_kmers * 8 / 1e9),
+                "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                "index_build_s": round(build_s, 2), "index_load_s": round(load_s, 2),
+            },
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": f"of {peak_kind}",
+                         "kernel": "search_kernel", "kernel_ms": kern_ms, "bytes_per_kmer_model": b_kmer,
+                         "mean_steps": mean_steps},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    ix.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def reference_arm(args, k, p):
+    import oracle as orc
+    import sbwt_gpu_b200 as sg
+    genome, letters, rows = workload(args.scale, 0)
+    built = sg.build_sbwt([genome.tobytes()], k)
+    ox = orc.OracleIndex(built.bits, built.n_bits)
+    del built
+    table = ox.presearch(p) if p else None
+    # each step: a bounded sample of the batch sized to ~budget seconds
+    budget = max(1.0, min(args.cpu_seconds, 150.0 / max(args.steps + args.warmup, 1)))
+    rate, ans, steps, nr, threads = cpu_reference(ox, letters, rows, k, p, budget, table)
+    sub_rows = rows[: nr + 1]
+    sub_letters = letters[: int(sub_rows[-1])]
+    for _ in range(max(args.warmup - 1, 0)):
+        ox.search_reads(sub_letters, sub_rows, k, p, table)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        ox.search_reads(sub_letters, sub_rows, k, p, table)
+    dt = time.perf_counter() - t
+    value = ans.size * args.steps / dt
+    sample = (f"first {nr} reads ({ans.size} k-mers) per step of the large workload; C restatement of the "
+              f"reference search (the reference has no CPU search), OpenMP, {threads} threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded)",
+        "config": {"workload": "large: 100 Mbp genome (41% GC) + 5% repeats, SBWT k=31, p=12, "
+                               "10M reads x 150 bp (10% genome-sampled with 1% subs, 90% random)", "k": k, "p": p},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,236 @@
+/*
+ * sbwt_gpu.h -- C ABI of the B200 (sm_100a) SBWT k-mer search engine.
+ *
+ * The engine is a drop-in for the search path of epicharri/sbwt_gpu
+ * (plain-matrix SBWT index -> poppy rank structures -> presearch table ->
+ * query ingest -> per-k-mer search -> answers).  Each entry point below names
+ * the reference interface it replaces (paths relative to the reference root).
+ *
+ * Conventions, as in the reference (include/gpu/cuda.hpp:7-13):
+ *   - every `int` entry point returns 0 on success and non-zero on error;
+ *     sbwt_last_error() gives the message of the last failure on this thread;
+ *   - answers are u64: the colex rank of the k-mer's SBWT node, or
+ *     0xFFFFFFFFFFFFFFFF (printed as -1) when the k-mer is absent
+ *     (include/gpu/search_kernel.hpp:98-103);
+ *   - the caller owns the buffers it passes; an sbwt_index owns the index,
+ *     its rank layouts and its presearch table;
+ *   - calls that take a `stream` are ordered on that cudaStream_t (passed as
+ *     void*, NULL = the legacy default stream); one index may be used by one
+ *     host thread at a time.
+ * There is no CPU fallback: without a usable CUDA device every compute entry
+ * point fails with an error.
+ */
+#ifndef SBWT_GPU_H
+#define SBWT_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SBWT_GPU_ABI_VERSION 1
+
+/* Rank-structure kinds of the reference (include/enums.hpp:9-11). */
+#define SBWT_POPPY 1
+#define SBWT_CUM_POPPY 2
+
+/* Search layouts of this engine. */
+#define SBWT_LAYOUT_LINES 0 /* 32-byte lines: 32-bit rank word + 224 bits (default) */
+#define SBWT_LAYOUT_POPPY 1 /* the reference's L0/L12 poppy layout (bits_in_superblock, rank_structure) */
+
+typedef struct sbwt_index sbwt_index;
+
+/* Run parameters.  Replaces epic::Parameters (include/parameters.hpp:39-63);
+ * field names follow its members, defaults follow its initialisers. */
+typedef struct {
+    uint32_t k;                  /* k-mer length, 3..32 (parameters.hpp:49, default 30) */
+    uint32_t k_presearch;        /* presearch depth p, 0 = without presearch (parameters.hpp:50) */
+    uint32_t bits_in_superblock; /* 256|512|1024|2048|4096 (parameters.hpp:42) */
+    int32_t rank_structure;      /* SBWT_POPPY | SBWT_CUM_POPPY (parameters.hpp:47) */
+    int32_t with_shuffles;       /* cooperative rank for the poppy layout (parameters.hpp:45) */
+    uint32_t threads_per_block;  /* 0 = engine default (parameters.hpp:51) */
+    int32_t device;              /* CUDA device ordinal (the reference uses 0, parameters.hpp:81) */
+    int32_t layout;              /* SBWT_LAYOUT_LINES | SBWT_LAYOUT_POPPY */
+    uint32_t kmers_per_thread;   /* search kernel: k-mer slots per thread, 1..8 (0 = default) */
+    uint32_t threads_per_kmer;   /* search kernel: lanes sharing one k-mer, 1|2|4 (0 = default) */
+} sbwt_params;
+
+/* Fills the defaults (k=30, p=12, SB=1024, poppy, no shuffles, device 0,
+ * line layout).  No reference counterpart (the reference uses member
+ * initialisers, parameters.hpp:41-56). */
+int sbwt_params_default(sbwt_params *params);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *sbwt_last_error(void);
+
+/* ------------------------------------------------------------------ index */
+
+/* Loads the four A/C/G/T bit-vector files (u64 little-endian bit count, then
+ * ceil(n/8) bytes, position p at byte 8+p/8, bit 7-p%8), builds the rank
+ * structures on the GPU, the C array, and the presearch table for
+ * params->k_presearch.  Replaces epic::MatrixSBWT::create
+ * (include/matrix_sbwt.hpp:32-200) with BitVector::create/read
+ * (include/bit_vector.hpp:65-138) and RankDataStructures
+ * (include/rank_data_structures.hpp:59-198). */
+int sbwt_index_load(const char *file_a, const char *file_c, const char *file_g, const char *file_t,
+                    const sbwt_params *params, sbwt_index **out);
+
+/* Same from host memory: bits[c] holds n_bits bits of vector c in the
+ * reference's in-memory word layout (position p at bit 63-p%64 of word p/64,
+ * i.e. after the byte swap of rank_data_structures.hpp:98).  Used by the
+ * builder and the tests.  No file-level counterpart in the reference. */
+int sbwt_index_from_host(const uint64_t *const bits[4], uint64_t n_bits, const sbwt_params *params,
+                         sbwt_index **out);
+
+void sbwt_index_free(sbwt_index *index);
+
+/* Number of SBWT columns n and the C array (counts_before,
+ * matrix_sbwt.hpp:150-157). */
+int sbwt_index_info(const sbwt_index *index, uint64_t *n_bits, uint64_t C[5], uint32_t *k, uint32_t *k_presearch);
+
+/* (Re)builds the presearch table for depth p (0 frees it: search without
+ * presearch).  Replaces epic::PreSearch::call_presearch
+ * (include/presearch.hpp:32-130) and the presearch kernel
+ * (include/gpu/presearch_kernel.hpp:19-37). */
+int sbwt_presearch(sbwt_index *index, uint32_t p);
+
+/* Copies the presearch table to the host in the reference's format: two
+ * arrays node_lefts[4^p], node_rights[4^p] (include/gpu/device_memory.hpp:
+ * 136-138). */
+int sbwt_presearch_export(const sbwt_index *index, uint64_t *node_lefts, uint64_t *node_rights, uint64_t count);
+
+/* Rebuilds the poppy rank structures on the GPU for (bits_in_superblock,
+ * rank_structure) and copies L0 and L12 of vector c (0..3) to the host:
+ * sizes are 1 + (n >> (SB==4096 ? 31 : 32)) and 1 + ceil(n/SB) words.
+ * Replaces RankDataStructures::construct (rank_data_structures.hpp:142-198). */
+int sbwt_rank_export(sbwt_index *index, uint32_t bits_in_superblock, int32_t rank_structure, int c,
+                     uint64_t *L0, uint64_t l0_words, uint64_t *L12, uint64_t l12_words);
+
+/* Selects the search layout / kernel shape for later searches (building the
+ * poppy structures if needed).  No reference counterpart: the reference
+ * picks these by template switch (include/epicseq/search_caller.hpp:81-209). */
+int sbwt_configure(sbwt_index *index, int32_t layout, uint32_t bits_in_superblock, int32_t rank_structure,
+                   int32_t with_shuffles, uint32_t kmers_per_thread, uint32_t threads_per_kmer,
+                   uint32_t threads_per_block);
+
+/* ----------------------------------------------------------------- search */
+
+/* The reference kernel contract: d_kmer_string holds the packed letters
+ * (n_words u64, 32 letters per word, letter j of a word at bits 63-2j..62-2j,
+ * with at least one word of padding after the last letter);
+ * d_positions_in_results_out[j] holds the letter offset of k-mer j on entry
+ * and its answer on return (in place).  All pointers are device pointers.
+ * Replaces epic::gpu::launch_search_kernel / search
+ * (include/gpu/search_and_presearch_launchers.hpp:21-60,
+ *  include/gpu/search_kernel.hpp:61-104).  Unlike the reference, no thread
+ * runs past n_kmers. */
+int sbwt_search_packed(sbwt_index *index, const uint64_t *d_kmer_string, uint64_t n_words,
+                       uint64_t *d_positions_in_results_out, uint64_t n_kmers, void *stream);
+
+/* 2-bit packs n_letters ASCII letters (device) into d_words (device,
+ * ceil((n_letters+32)/32) words; letters past n_letters are packed as A).
+ * Mapping A/a->0 C/c->1 G/g->2 T/t->3, every other byte -> 0.  Replaces
+ * create_kmer_string (include/gpu/create_kmer_string.hpp:22-42). */
+int sbwt_pack(const uint8_t *d_letters, uint64_t n_letters, uint64_t *d_words, void *stream);
+
+/* Searches every k-mer of a batch of reads held on the device:
+ * d_letters = concatenated reads (n_letters bytes), d_row_starts[r] = offset
+ * of read r (n_rows + 1 entries, last = n_letters).  K-mers never cross a
+ * read boundary; a read shorter than k has no k-mers.  Writes one answer per
+ * k-mer, reads in order, to d_answers (device, n_kmers entries, n_kmers =
+ * sum of max(0, len-k+1)).  d_member_bits (optional, device, ceil(n_kmers/
+ * 32) u32 words) receives bit j%32 of word j/32 = (answer j != -1).
+ * Replaces the chain KmerSearch::parse_kmer_string_in_gpu ->
+ * create_positions_in_gpu -> call_search (include/epicseq/kmer_search.hpp:
+ * 97-185) with one pack kernel and one persistent work-stealing search
+ * kernel; no per-k-mer positions array is materialised. */
+int sbwt_search_reads(sbwt_index *index, const uint8_t *d_letters, uint64_t n_letters, const uint64_t *d_row_starts,
+                      uint64_t n_rows, uint64_t *d_answers, uint32_t *d_member_bits, uint64_t n_kmers, void *stream);
+
+/* Host-memory form of sbwt_search_reads: letters, row starts and answers
+ * are host buffers (pinned or pageable).  The batch is streamed through the
+ * GPU in chunks with copies overlapped with compute.  Replaces the
+ * parse/position/search/copy-back chain of KmerSearch::search
+ * (kmer_search.hpp:97-160) and ResultsPersister's device-to-host copy
+ * (results_persister.hpp:58-65). */
+int sbwt_search_reads_host(sbwt_index *index, const uint8_t *letters, uint64_t n_letters, const uint64_t *row_starts,
+                           uint64_t n_rows, uint64_t *answers, uint64_t n_kmers);
+
+/* Kernel timing of the last sbwt_search_reads call on this index, from CUDA
+ * events recorded on that call's stream around each phase (enabled with
+ * sbwt_profile_enable; reading synchronizes on the last event).  The
+ * reference times its kernels the same way (include/gpu/device_stream.hpp:
+ * 52-86, search_and_presearch_launchers.hpp:41,53-54). */
+typedef struct {
+    float pack_ms;      /* 2-bit packing */
+    float table_ms;     /* per-row k-mer table (scan) and chunk table */
+    float search_ms;    /* the search kernel */
+    float member_ms;    /* membership bitmap (0 if not requested) */
+    uint32_t launches;  /* kernels launched by the call */
+    uint32_t search_blocks; /* grid of the persistent search kernel */
+} sbwt_profile;
+
+int sbwt_profile_enable(sbwt_index *index, int on);
+int sbwt_profile_read(sbwt_index *index, sbwt_profile *out);
+
+/* Number of k-mers in a batch of rows (sum of max(0, len-k+1)). */
+uint64_t sbwt_count_kmers(const uint64_t *row_starts, uint64_t n_rows, uint32_t k);
+
+/* ------------------------------------------------------------ query files */
+
+/* Reads a FASTA query file the way KmerSearch::read_file does
+ * (include/epicseq/kmer_search.hpp:319-342): every line that does not start
+ * with '>' is one read; letters are concatenated.  Divergence: a last line
+ * without '\n' keeps its last letter.  The returned buffers are owned by
+ * the library (free with sbwt_queries_free). */
+typedef struct {
+    uint8_t *letters;     /* n_letters bytes (+32 zero bytes of padding) */
+    uint64_t n_letters;
+    uint64_t *row_starts; /* n_rows + 1 entries */
+    uint64_t n_rows;
+    uint64_t n_kmers;     /* for the k given to sbwt_queries_read */
+} sbwt_queries;
+
+int sbwt_queries_read(const char *path, uint32_t k, sbwt_queries *out);
+void sbwt_queries_free(sbwt_queries *q);
+
+/* Formats answers as the reference prints them (results_persister.hpp:82-95):
+ * per read, each answer as a signed int64 followed by one space, then '\n'
+ * (a read shorter than k gives an empty line).  Writes to `out` (size cap);
+ * returns the number of bytes, or -1 if cap is too small (call with
+ * out == NULL for the exact size). */
+int64_t sbwt_format_answers(const uint64_t *row_starts, uint64_t n_rows, uint32_t k, const uint64_t *answers,
+                            char *out, uint64_t cap);
+
+/* -------------------------------------------------------------- builder */
+
+/* Builds the plain-matrix SBWT of every k-mer of the given sequences
+ * (forward strand; k-mers holding a byte other than ACGTacgt are skipped),
+ * with dummy nodes for source k-mers, in the reference's matrix format.
+ * seqs = concatenated sequences, seq_starts = n_seqs + 1 offsets.
+ * Outputs: *n_bits = number of columns (nodes), bits[c] (library-owned,
+ * ceil(n/64) words each, reference in-memory layout), free with
+ * sbwt_build_free.  The reference relies on an external tool for this step;
+ * this builder is this project's own. */
+typedef struct {
+    uint64_t n_bits;
+    uint64_t n_kmers;   /* distinct k-mers */
+    uint64_t n_dummies; /* dummy nodes including the root */
+    uint64_t *bits[4];
+    uint64_t n_words;
+} sbwt_built;
+
+int sbwt_build(const uint8_t *seqs, const uint64_t *seq_starts, uint64_t n_seqs, uint32_t k, sbwt_built *out);
+void sbwt_build_free(sbwt_built *b);
+
+/* Writes vector c of a built index to `path` in the reference file format
+ * (include/bit_vector.hpp:65-128). */
+int sbwt_write_bitvector(const char *path, const uint64_t *bits, uint64_t n_bits);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SBWT_GPU_H */

@@ -1,0 +1,257 @@
+"""sbwt_gpu_b200 -- B200 (sm_100a) k-mer membership engine over the Spectral
+Burrows-Wheeler Transform, a drop-in for the search path of epicharri/sbwt_gpu.
+
+The engine is C++/CUDA behind the C ABI of ``include/sbwt_gpu.h``
+(``libsbwt_gpu.so``, plus the ``sbwt_search`` command-line tool).  This module
+is a thin ctypes layer over that ABI for tests, benchmarks and Python callers;
+it does no compute of its own.  Names follow the reference:
+
+* ``Index.load``         <- epic::MatrixSBWT::create (include/matrix_sbwt.hpp:32-200)
+* ``Index.presearch``    <- epic::PreSearch::call_presearch (include/presearch.hpp:32-130)
+* ``Index.search_packed``<- epic::gpu::launch_search_kernel (include/gpu/search_and_presearch_launchers.hpp:21-60)
+* ``read_queries``       <- epic::KmerSearch::read_file (include/epicseq/kmer_search.hpp:319-342)
+* ``format_answers``     <- epic::ResultsPersister::save_results_to_file (include/epicseq/results_persister.hpp:82-95)
+"""
+import ctypes
+import os
+from ctypes import POINTER, byref, c_uint32, c_uint64, c_void_p
+
+import numpy as np
+
+from ._lib import (CLI_PATH, LIB_PATH, SBWT_CUM_POPPY, SBWT_LAYOUT_LINES, SBWT_LAYOUT_POPPY, SBWT_POPPY, Built,
+                   Params, Profile, Queries, SbwtError, check, lib)
+
+__all__ = [
+    "Index", "Params", "SbwtError", "build_sbwt", "write_index_files", "read_queries", "format_answers",
+    "count_kmers", "default_params", "SBWT_POPPY", "SBWT_CUM_POPPY", "SBWT_LAYOUT_LINES", "SBWT_LAYOUT_POPPY",
+    "LIB_PATH", "CLI_PATH", "NOT_FOUND",
+]
+
+NOT_FOUND = 0xFFFFFFFFFFFFFFFF  # answer of an absent k-mer (printed as -1)
+
+
+def default_params(**kw):
+    """``sbwt_params`` with the reference's defaults (parameters.hpp:41-56), overridden by ``kw``."""
+    p = Params()
+    check(lib.sbwt_params_default(byref(p)))
+    for key, val in kw.items():
+        if not hasattr(p, key):
+            raise TypeError(f"unknown parameter {key}")
+        setattr(p, key, val)
+    return p
+
+
+def _ptr(a):
+    """Data pointer of a numpy array or a torch tensor (host or device)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return c_void_p(a.ctypes.data)
+    return c_void_p(a.data_ptr())
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        return None
+    return c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+
+
+class Index:
+    """An SBWT index resident on one GPU (``sbwt_index*``)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    # -------------------------------------------------------------- creation
+    @classmethod
+    def load(cls, file_a, file_c, file_g, file_t, params=None, **kw):
+        p = params if params is not None else default_params(**kw)
+        h = c_void_p()
+        check(lib.sbwt_index_load(os.fsencode(file_a), os.fsencode(file_c), os.fsencode(file_g),
+                                  os.fsencode(file_t), byref(p), byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_bits(cls, bits, n_bits, params=None, **kw):
+        """bits: four uint64 arrays (reference in-memory layout: position p at bit 63-p%64 of word p/64)."""
+        p = params if params is not None else default_params(**kw)
+        arrs = [np.ascontiguousarray(b, dtype=np.uint64) for b in bits]
+        need = (int(n_bits) + 63) // 64
+        for a in arrs:
+            if a.size < need:
+                raise ValueError(f"a bit vector holds {a.size} words, {need} needed")
+        ptrs = (c_void_p * 4)(*[a.ctypes.data for a in arrs])
+        h = c_void_p()
+        check(lib.sbwt_index_from_host(ptrs, int(n_bits), byref(p), byref(h)))
+        return cls(h)
+
+    def close(self):
+        if self._h:
+            lib.sbwt_index_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ------------------------------------------------------------ inspection
+    def info(self):
+        n = c_uint64()
+        C = (c_uint64 * 5)()
+        k = c_uint32()
+        p = c_uint32()
+        check(lib.sbwt_index_info(self._h, byref(n), C, byref(k), byref(p)))
+        return {"n_bits": n.value, "C": [int(x) for x in C], "k": k.value, "k_presearch": p.value}
+
+    def presearch(self, p):
+        check(lib.sbwt_presearch(self._h, int(p)))
+
+    def presearch_table(self):
+        p = self.info()["k_presearch"]
+        if p == 0:
+            raise SbwtError("the index has no presearch table")
+        count = 1 << (2 * p)
+        lefts = np.empty(count, dtype=np.uint64)
+        rights = np.empty(count, dtype=np.uint64)
+        check(lib.sbwt_presearch_export(self._h, _ptr(lefts), _ptr(rights), count))
+        return lefts, rights
+
+    def rank_structures(self, bits_in_superblock, rank_structure, c):
+        n = self.info()["n_bits"]
+        log_h = 31 if bits_in_superblock == 4096 else 32
+        l0w = 1 + (n >> log_h)
+        l12w = 1 + ((n + bits_in_superblock - 1) // bits_in_superblock)
+        L0 = np.empty(l0w, dtype=np.uint64)
+        L12 = np.empty(l12w, dtype=np.uint64)
+        check(lib.sbwt_rank_export(self._h, bits_in_superblock, rank_structure, c, _ptr(L0), l0w, _ptr(L12), l12w))
+        return L0, L12
+
+    def configure(self, layout=SBWT_LAYOUT_LINES, bits_in_superblock=1024, rank_structure=SBWT_POPPY,
+                  with_shuffles=0, kmers_per_thread=0, threads_per_kmer=0, threads_per_block=0):
+        check(lib.sbwt_configure(self._h, layout, bits_in_superblock, rank_structure, int(with_shuffles),
+                                 kmers_per_thread, threads_per_kmer, threads_per_block))
+
+    def profile(self, on=True):
+        """Enables CUDA-event timing of each sbwt_search_reads phase."""
+        check(lib.sbwt_profile_enable(self._h, int(on)))
+
+    def last_profile(self):
+        pr = Profile()
+        check(lib.sbwt_profile_read(self._h, byref(pr)))
+        return {"pack_ms": pr.pack_ms, "table_ms": pr.table_ms, "search_ms": pr.search_ms,
+                "member_ms": pr.member_ms, "launches": pr.launches, "search_blocks": pr.search_blocks}
+
+    # ---------------------------------------------------------------- search
+    def search_packed(self, d_words, d_positions, n_kmers=None, stream=None):
+        """Reference kernel contract: positions in, answers out, in place (device tensors, 64-bit)."""
+        n = int(d_positions.numel()) if n_kmers is None else int(n_kmers)
+        check(lib.sbwt_search_packed(self._h, _ptr(d_words), int(d_words.numel()), _ptr(d_positions), n,
+                                     _stream_ptr(stream)))
+
+    def search_reads(self, d_letters, d_row_starts, d_answers, n_kmers, d_member_bits=None, stream=None):
+        """Device-resident reads (uint8 letters, int64 row starts) -> device answers."""
+        n_rows = int(d_row_starts.numel()) - 1
+        check(lib.sbwt_search_reads(self._h, _ptr(d_letters), int(d_letters.numel()), _ptr(d_row_starts), n_rows,
+                                    _ptr(d_answers), _ptr(d_member_bits), int(n_kmers), _stream_ptr(stream)))
+
+    def search_reads_host(self, letters, row_starts, answers=None):
+        """Host reads -> host answers (numpy), streamed through the GPU."""
+        letters = np.ascontiguousarray(letters, dtype=np.uint8) if isinstance(letters, np.ndarray) else letters
+        rs = row_starts
+        n_rows = (rs.size if isinstance(rs, np.ndarray) else rs.numel()) - 1
+        if isinstance(rs, np.ndarray):
+            rs = np.ascontiguousarray(rs, dtype=np.uint64)
+            nk = int(lib.sbwt_count_kmers(_ptr(rs), n_rows, self.info()["k"]))
+        else:
+            nk = count_kmers(rs.numpy().view(np.uint64), self.info()["k"])
+        if answers is None:
+            answers = np.empty(max(nk, 1), dtype=np.uint64)
+        n_letters = letters.size if isinstance(letters, np.ndarray) else letters.numel()
+        check(lib.sbwt_search_reads_host(self._h, _ptr(letters), int(n_letters), _ptr(rs), n_rows, _ptr(answers), nk))
+        return answers[:nk] if isinstance(answers, np.ndarray) else answers
+
+
+# ------------------------------------------------------------------ builder
+
+class BuiltIndex:
+    """Bit vectors of an SBWT built on the host (reference in-memory word layout)."""
+
+    def __init__(self, bits, n_bits, n_kmers, n_dummies):
+        self.bits = bits
+        self.n_bits = n_bits
+        self.n_kmers = n_kmers
+        self.n_dummies = n_dummies
+
+
+def _as_letters_and_starts(seqs):
+    if isinstance(seqs, tuple):
+        letters, starts = seqs
+        return np.ascontiguousarray(letters, dtype=np.uint8), np.ascontiguousarray(starts, dtype=np.uint64)
+    parts = [np.frombuffer(s.encode() if isinstance(s, str) else bytes(s), dtype=np.uint8) for s in seqs]
+    starts = np.zeros(len(parts) + 1, dtype=np.uint64)
+    starts[1:] = np.cumsum([p.size for p in parts])
+    letters = np.concatenate(parts) if parts else np.zeros(0, dtype=np.uint8)
+    return letters, starts
+
+
+def build_sbwt(seqs, k):
+    """Builds the plain-matrix SBWT of all k-mers of ``seqs`` (list of str/bytes, or (letters, starts))."""
+    letters, starts = _as_letters_and_starts(seqs)
+    b = Built()
+    check(lib.sbwt_build(_ptr(letters), _ptr(starts), starts.size - 1, int(k), byref(b)))
+    try:
+        bits = [np.ctypeslib.as_array(b.bits[c], shape=(b.n_words,)).copy() for c in range(4)]
+    finally:
+        lib.sbwt_build_free(byref(b))
+    return BuiltIndex(bits, int(b.n_bits), int(b.n_kmers), int(b.n_dummies))
+
+
+def write_index_files(prefix, built):
+    """Writes ``prefix``.A/.C/.G/.T in the reference's bit-vector file format."""
+    paths = []
+    for c, ch in enumerate("ACGT"):
+        path = f"{prefix}.{ch}"
+        check(lib.sbwt_write_bitvector(os.fsencode(path), _ptr(built.bits[c]), built.n_bits))
+        paths.append(path)
+    return paths
+
+
+# ------------------------------------------------------------------ queries
+
+def read_queries(path, k):
+    """FASTA reads as the reference reads them: (letters uint8, row_starts uint64, n_kmers)."""
+    q = Queries()
+    check(lib.sbwt_queries_read(os.fsencode(path), int(k), byref(q)))
+    try:
+        letters = np.ctypeslib.as_array(q.letters, shape=(q.n_letters + 32,))[: q.n_letters].copy() \
+            if q.n_letters else np.zeros(0, dtype=np.uint8)
+        rows = np.ctypeslib.as_array(q.row_starts, shape=(q.n_rows + 1,)).copy()
+        nk = int(q.n_kmers)
+    finally:
+        lib.sbwt_queries_free(byref(q))
+    return letters, rows, nk
+
+
+def count_kmers(row_starts, k):
+    rs = np.ascontiguousarray(row_starts, dtype=np.uint64)
+    return int(lib.sbwt_count_kmers(_ptr(rs), rs.size - 1, int(k)))
+
+
+def format_answers(row_starts, k, answers):
+    """The reference's stdout text for the answers of the given rows (bytes)."""
+    rs = np.ascontiguousarray(row_starts, dtype=np.uint64)
+    ans = np.ascontiguousarray(answers, dtype=np.uint64)
+    size = lib.sbwt_format_answers(_ptr(rs), rs.size - 1, int(k), _ptr(ans), None, 0)
+    buf = ctypes.create_string_buffer(int(size) + 1)
+    got = lib.sbwt_format_answers(_ptr(rs), rs.size - 1, int(k), _ptr(ans), buf, int(size) + 1)
+    if got < 0:
+        raise SbwtError("format buffer too small")
+    return buf.raw[:got]

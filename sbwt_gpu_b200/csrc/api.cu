@@ -1,0 +1,495 @@
+// api.cu -- the C ABI (include/sbwt_gpu.h): index handle, device memory,
+// streams, and the search entry points.
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "device.cuh"
+#include "internal.h"
+
+using sbwt::set_error;
+using sbwt::u32;
+using sbwt::u64;
+
+namespace sbwt {
+
+void Workspace::release() {
+    cudaFree(words); cudaFree(kstart); cudaFree(chunk_row); cudaFree(scan); cudaFree(counter);
+    cudaFree(letters); cudaFree(rows); cudaFree(answers);
+    if (h_rows) cudaFreeHost(h_rows);
+    if (h_letters) cudaFreeHost(h_letters);
+    if (h_answers) cudaFreeHost(h_answers);
+    *this = Workspace();
+}
+
+// Grow-only device buffer of `need` elements.
+template <class T>
+int grow(T *&p, size_t &cap, size_t need) {
+    if (cap >= need && p) return 0;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    const size_t want = std::max(need, (size_t)1);
+    SBWT_CHECK_CUDA(cudaMalloc((void **)&p, want * sizeof(T)));
+    cap = want;
+    return 0;
+}
+
+// Grow-only pinned host buffer of `need` elements.
+template <class T>
+int grow_host(T *&p, size_t &cap, size_t need) {
+    if (cap >= need && p) return 0;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    const size_t want = std::max(need, (size_t)1);
+    SBWT_CHECK_CUDA(cudaHostAlloc((void **)&p, want * sizeof(T), cudaHostAllocDefault));
+    cap = want;
+    return 0;
+}
+
+template int grow<uint8_t>(uint8_t *&, size_t &, size_t);
+template int grow<uint64_t>(uint64_t *&, size_t &, size_t);
+template int grow_host<uint8_t>(uint8_t *&, size_t &, size_t);
+template int grow_host<uint64_t>(uint64_t *&, size_t &, size_t);
+
+namespace {
+
+int use_device(int device) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0)
+        return set_error("no CUDA device is available (%s); this engine has no CPU fallback",
+                         e != cudaSuccess ? cudaGetErrorString(e) : "0 devices");
+    if (device < 0 || device >= count) return set_error("CUDA device %d does not exist (%d devices)", device, count);
+    SBWT_CHECK_CUDA(cudaSetDevice(device));
+    return 0;
+}
+
+int validate_params(const sbwt_params *p) {
+    if (p->k < 3 || p->k > 32) return set_error("The value of k must be at least 3 and at most 32.");
+    if (p->k_presearch > p->k) return set_error("presearch depth %u exceeds k = %u", p->k_presearch, p->k);
+    return 0;
+}
+
+void apply_shape(sbwt_index *ix, const sbwt_params *p) {
+    sbwt::KernelShape &sh = ix->shape;
+    sh.layout = p->layout == SBWT_LAYOUT_POPPY ? SBWT_LAYOUT_POPPY : SBWT_LAYOUT_LINES;
+    sh.kpt = p->kmers_per_thread ? p->kmers_per_thread : 4;
+    sh.tpk = p->threads_per_kmer ? p->threads_per_kmer : 1;
+    sh.tpb = p->threads_per_block ? std::min<u32>(p->threads_per_block, 256u) : 256u;
+    sh.sb = p->bits_in_superblock;
+    sh.kind = p->rank_structure;
+    sh.shuffles = p->with_shuffles;
+}
+
+// Shared tail of the two index constructors: `words[c]` hold ceil(n/64)
+// words of vector c in the reference's in-memory layout.
+int finish_index(sbwt_index *ix, const u64 *const words[4], const sbwt_params *prm) {
+    const u64 n = ix->n;
+    const u64 nw = (n + 63) / 64;
+    ix->wpv = (n + 4095) / 4096 * 64 + 64;  // bit_vector.hpp:104 plus one spare block
+    SBWT_CHECK_CUDA(cudaMalloc(&ix->d_bits, 4 * ix->wpv * sizeof(u64)));
+    SBWT_CHECK_CUDA(cudaMemset(ix->d_bits, 0, 4 * ix->wpv * sizeof(u64)));
+    for (int c = 0; c < 4; c++) {
+        u64 *dst = ix->d_bits + (u64)c * ix->wpv;
+        if (nw > 1) SBWT_CHECK_CUDA(cudaMemcpy(dst, words[c], (nw - 1) * sizeof(u64), cudaMemcpyHostToDevice));
+        // bits past n are zero on the device whatever the caller's padding holds
+        u64 last = words[c][nw - 1];
+        if (n % 64) last &= ~0ull << (64 - n % 64);
+        SBWT_CHECK_CUDA(cudaMemcpy(dst + nw - 1, &last, sizeof(u64), cudaMemcpyHostToDevice));
+    }
+    cudaStream_t s = 0;
+    u64 ones[4] = {0, 0, 0, 0};
+    if (n / sbwt::dev::kLineBits + 1 <= sbwt::dev::kMaxLinesPerChar) {
+        ix->lpc = (u32)(((n / sbwt::dev::kLineBits + 1) + 7) / 8 * 8);
+        SBWT_CHECK_CUDA(cudaMalloc(&ix->d_lines, 4ull * ix->lpc * sizeof(ulonglong4)));
+        SBWT_TRY(sbwt::build_lines(ix, s, ones));
+        ix->lines_ok = true;
+    }
+    const bool want_poppy = prm->layout == SBWT_LAYOUT_POPPY || !ix->lines_ok;
+    if (want_poppy) {
+        SBWT_TRY(sbwt::build_poppy(ix, prm->bits_in_superblock, prm->rank_structure, s));
+        if (!ix->lines_ok) {
+            // ones of each vector = sum of the last L12 relative count chain: read via the sentinel
+            std::vector<u64> l0(ix->l0w), l12(1);
+            for (int c = 0; c < 4; c++) {
+                SBWT_CHECK_CUDA(cudaMemcpy(l0.data(), ix->d_L0 + (u64)c * ix->l0w, ix->l0w * sizeof(u64),
+                                           cudaMemcpyDeviceToHost));
+                SBWT_CHECK_CUDA(cudaMemcpy(l12.data(), ix->d_L12 + (u64)c * ix->l12w + ix->l12w - 1, sizeof(u64),
+                                           cudaMemcpyDeviceToHost));
+                const u64 nsb = ix->l12w - 1;
+                u64 h = (nsb * ix->sb) >> (ix->sb == 4096 ? 31 : 32);
+                if (h >= ix->l0w) h = ix->l0w - 1;
+                ones[c] = l0[h] + (l12[0] >> (ix->sb == 4096 ? 33 : 32));
+            }
+        }
+    }
+    // matrix_sbwt.hpp:150-157
+    ix->C[0] = 1;
+    for (int c = 0; c < 4; c++) ix->C[c + 1] = ix->C[c] + ones[c];
+    if (ix->C[4] != n)
+        return set_error("the bit vectors are not an SBWT: 1 + total ones = %llu but n = %llu",
+                         (unsigned long long)ix->C[4], (unsigned long long)n);
+    apply_shape(ix, prm);
+    if (ix->shape.layout == SBWT_LAYOUT_LINES && !ix->lines_ok) ix->shape.layout = SBWT_LAYOUT_POPPY;
+    SBWT_TRY(sbwt::run_presearch(ix, prm->k_presearch, s));
+    SBWT_CHECK_CUDA(cudaDeviceSynchronize());
+    return 0;
+}
+
+int new_index(const sbwt_params *prm, sbwt_index **out, sbwt_index **ix_out) {
+    if (!out) return set_error("out is NULL");
+    *out = nullptr;
+    sbwt_params def;
+    sbwt_params_default(&def);
+    if (!prm) prm = &def;
+    SBWT_TRY(validate_params(prm));
+    SBWT_TRY(use_device(prm->device));
+    sbwt_index *ix = new (std::nothrow) sbwt_index();
+    if (!ix) return set_error("out of host memory");
+    ix->device = prm->device;
+    ix->k = prm->k;
+    cudaDeviceGetAttribute(&ix->num_sms, cudaDevAttrMultiProcessorCount, prm->device);
+    if (ix->num_sms <= 0) ix->num_sms = 1;
+    *ix_out = ix;
+    return 0;
+}
+
+// BitVector::create header checks (include/bit_vector.hpp:65-109).
+int read_vector(const char *path, u64 &n_bits, std::vector<u64> &words) {
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return set_error("The file %s can not be opened.", path);
+    std::fseek(f, 0, SEEK_END);
+    const long size = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    if (size < 8) {
+        std::fclose(f);
+        return set_error("The size of the file %s is too small to contain any data.", path);
+    }
+    unsigned char hdr[8];
+    if (std::fread(hdr, 1, 8, f) != 8) {
+        std::fclose(f);
+        return set_error("The file %s can not be read.", path);
+    }
+    u64 n = 0;
+    for (int i = 0; i < 8; i++) n |= (u64)hdr[i] << (8 * i);
+    if (n == 0) {
+        std::fclose(f);
+        return set_error("The first 8 bytes in the file %s indicates that there is a bit vector of size 0 in the file.",
+                         path);
+    }
+    const u64 nbytes = (n + 7) / 8;
+    if ((u64)size - 8 < nbytes) {
+        std::fclose(f);
+        return set_error("The file %s holds %llu data bytes; its header announces %llu bits (%llu bytes).", path,
+                         (unsigned long long)((u64)size - 8), (unsigned long long)n, (unsigned long long)nbytes);
+    }
+    words.assign((n + 63) / 64, 0ull);
+    const size_t got = std::fread(words.data(), 1, nbytes, f);
+    std::fclose(f);
+    if (got != nbytes) return set_error("The file %s can not be read.", path);
+    // byte swap (rank_data_structures.hpp:98,103-113): position p at bit 63 - p%64
+    const int64_t nw = (int64_t)words.size();
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < nw; i++) words[i] = __builtin_bswap64(words[i]);
+    n_bits = n;
+    return 0;
+}
+
+}  // namespace
+}  // namespace sbwt
+
+using namespace sbwt;
+
+extern "C" int sbwt_params_default(sbwt_params *p) {
+    if (!p) return set_error("params is NULL");
+    std::memset(p, 0, sizeof(*p));
+    p->k = 30;                   // parameters.hpp:49
+    p->k_presearch = 12;         // parameters.hpp:50
+    p->bits_in_superblock = 1024;  // parameters.hpp:42
+    p->rank_structure = SBWT_POPPY;
+    p->with_shuffles = 0;
+    p->threads_per_block = 0;
+    p->device = 0;
+    p->layout = SBWT_LAYOUT_LINES;
+    p->kmers_per_thread = 0;
+    p->threads_per_kmer = 0;
+    return 0;
+}
+
+extern "C" int sbwt_index_from_host(const uint64_t *const bits[4], uint64_t n_bits, const sbwt_params *params,
+                                    sbwt_index **out) {
+    clear_error();
+    sbwt_params def;
+    sbwt_params_default(&def);
+    if (!params) params = &def;
+    if (n_bits == 0) return set_error("the index has no columns");
+    for (int c = 0; c < 4; c++)
+        if (!bits || !bits[c]) return set_error("bit vector %d is NULL", c);
+    sbwt_index *ix = nullptr;
+    SBWT_TRY(new_index(params, out, &ix));
+    ix->n = n_bits;
+    const int rc = finish_index(ix, bits, params);
+    if (rc) {
+        sbwt_index_free(ix);
+        return rc;
+    }
+    *out = ix;
+    return 0;
+}
+
+extern "C" int sbwt_index_load(const char *file_a, const char *file_c, const char *file_g, const char *file_t,
+                               const sbwt_params *params, sbwt_index **out) {
+    clear_error();
+    const char *files[4] = {file_a, file_c, file_g, file_t};
+    std::vector<u64> w[4];
+    u64 n[4] = {0, 0, 0, 0};
+    int rc[4] = {0, 0, 0, 0};
+    for (int c = 0; c < 4; c++) {
+        if (!files[c]) return set_error("bit vector file %d is NULL", c);
+    }
+    // the four files are read in parallel, as the reference's OpenMP tasks (matrix_sbwt.hpp:70-110)
+#pragma omp parallel for num_threads(4)
+    for (int c = 0; c < 4; c++) rc[c] = read_vector(files[c], n[c], w[c]);
+    for (int c = 0; c < 4; c++)
+        if (rc[c]) return set_error("%s", "a bit vector file could not be read (see the file checks)");
+    if (n[1] != n[0] || n[2] != n[0] || n[3] != n[0])  // matrix_sbwt.hpp:52-55
+        return set_error("The bit vectors have different lengths (%llu, %llu, %llu, %llu).", (unsigned long long)n[0],
+                         (unsigned long long)n[1], (unsigned long long)n[2], (unsigned long long)n[3]);
+    const u64 *ptrs[4] = {w[0].data(), w[1].data(), w[2].data(), w[3].data()};
+    return sbwt_index_from_host(ptrs, n[0], params, out);
+}
+
+extern "C" void sbwt_index_free(sbwt_index *ix) {
+    if (!ix) return;
+    cudaSetDevice(ix->device);
+    cudaFree(ix->d_bits);
+    cudaFree(ix->d_lines);
+    cudaFree(ix->d_L0);
+    cudaFree(ix->d_L12);
+    cudaFree(ix->d_pre);
+    cudaFree(ix->d_scan);
+    for (int i = 0; i < 2; i++) {
+        ix->ws[i].release();
+        if (ix->pipe_stream[i]) cudaStreamDestroy(ix->pipe_stream[i]);
+    }
+    for (auto &e : ix->prof_ev)
+        if (e) cudaEventDestroy(e);
+    delete ix;
+}
+
+extern "C" int sbwt_index_info(const sbwt_index *ix, uint64_t *n_bits, uint64_t C[5], uint32_t *k, uint32_t *p) {
+    clear_error();
+    if (!ix) return set_error("index is NULL");
+    if (n_bits) *n_bits = ix->n;
+    if (C) std::memcpy(C, ix->C, sizeof(ix->C));
+    if (k) *k = ix->k;
+    if (p) *p = ix->p;
+    return 0;
+}
+
+extern "C" int sbwt_presearch(sbwt_index *ix, uint32_t p) {
+    clear_error();
+    if (!ix) return set_error("index is NULL");
+    SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
+    return run_presearch(ix, p, 0);
+}
+
+extern "C" int sbwt_presearch_export(const sbwt_index *ix, uint64_t *lefts, uint64_t *rights, uint64_t count) {
+    clear_error();
+    if (!ix || !lefts || !rights) return set_error("NULL argument");
+    SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
+    return export_presearch(ix, lefts, rights, count);
+}
+
+extern "C" int sbwt_rank_export(sbwt_index *ix, uint32_t sb, int32_t kind, int c, uint64_t *L0, uint64_t l0_words,
+                                uint64_t *L12, uint64_t l12_words) {
+    clear_error();
+    if (!ix || !L0 || !L12) return set_error("NULL argument");
+    if (c < 0 || c > 3) return set_error("vector index must be 0..3");
+    SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
+    if (!ix->poppy_ok || ix->sb != sb || ix->kind != kind) SBWT_TRY(build_poppy(ix, sb, kind, 0));
+    if (l0_words != ix->l0w || l12_words != ix->l12w)
+        return set_error("rank export: expected %llu L0 and %llu L12 words", (unsigned long long)ix->l0w,
+                         (unsigned long long)ix->l12w);
+    SBWT_CHECK_CUDA(cudaMemcpy(L0, ix->d_L0 + (u64)c * ix->l0w, ix->l0w * sizeof(u64), cudaMemcpyDeviceToHost));
+    SBWT_CHECK_CUDA(cudaMemcpy(L12, ix->d_L12 + (u64)c * ix->l12w, ix->l12w * sizeof(u64), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+extern "C" int sbwt_configure(sbwt_index *ix, int32_t layout, uint32_t sb, int32_t kind, int32_t shuffles, uint32_t kpt,
+                              uint32_t tpk, uint32_t tpb) {
+    clear_error();
+    if (!ix) return set_error("index is NULL");
+    SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
+    if (layout == SBWT_LAYOUT_POPPY) {
+        if (!ix->poppy_ok || ix->sb != sb || ix->kind != kind) SBWT_TRY(build_poppy(ix, sb, kind, 0));
+    } else if (layout == SBWT_LAYOUT_LINES) {
+        if (!ix->lines_ok) return set_error("the line layout is not available for an index of %llu columns",
+                                            (unsigned long long)ix->n);
+    } else {
+        return set_error("unknown layout %d", layout);
+    }
+    if (tpb && (tpb % 32 || tpb > 256)) return set_error("threads_per_block must be a multiple of 32 up to 256");
+    if (kpt && !(kpt == 1 || kpt == 2 || kpt == 3 || kpt == 4 || kpt == 6 || kpt == 8))
+        return set_error("kmers_per_thread must be 1, 2, 3, 4, 6 or 8");
+    if (tpk && !(tpk == 1 || tpk == 2 || tpk == 4)) return set_error("threads_per_kmer must be 1, 2 or 4");
+    KernelShape &sh = ix->shape;
+    sh.layout = layout;
+    sh.sb = sb;
+    sh.kind = kind;
+    sh.shuffles = shuffles;
+    if (kpt) sh.kpt = kpt;
+    if (tpk) sh.tpk = tpk;
+    if (tpb) sh.tpb = tpb;
+    return 0;
+}
+
+namespace sbwt {
+namespace {
+
+SearchArgs base_args(const sbwt_index *ix) {
+    SearchArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.lines = ix->d_lines;
+    a.lpc = ix->lpc;
+    a.bits = ix->d_bits;
+    a.L0 = ix->d_L0;
+    a.L12 = ix->d_L12;
+    a.wpv = ix->wpv;
+    a.l0w = ix->l0w;
+    a.l12w = ix->l12w;
+    std::memcpy(a.C, ix->C, sizeof(a.C));
+    a.pre = ix->d_pre;
+    a.p = ix->p;
+    a.k = ix->k;
+    a.chunk = search_chunk(ix->shape);
+    return a;
+}
+
+}  // namespace
+
+// Device-resident batch of rows on stream s using workspace w.
+int search_rows_device(sbwt_index *ix, Workspace &w, const uint8_t *d_letters, u64 n_letters, const u64 *d_rows,
+                       u64 n_rows, u64 *d_answers, uint32_t *d_member, u64 n_kmers, cudaStream_t s) {
+    if (n_rows == 0 || n_kmers == 0) return 0;
+    const u64 n_words = (n_letters + 32 + 31) / 32;
+    SearchArgs a = base_args(ix);
+    SBWT_TRY(grow(w.words, w.words_cap, n_words));
+    SBWT_TRY(grow(w.kstart, w.kstart_cap, n_rows + 1));
+    SBWT_TRY(grow(w.scan, w.scan_cap, scan_scratch_words(n_rows)));
+    SBWT_TRY(grow(w.chunk_row, w.chunk_cap, (n_kmers + a.chunk - 1) / a.chunk));
+    SBWT_TRY(grow(w.counter, w.counter_cap, 1));
+    const bool prof = ix->prof_on;
+    if (prof) SBWT_CHECK_CUDA(cudaEventRecord(ix->prof_ev[0], s));
+    SBWT_TRY(launch_pack(d_letters, n_letters, w.words, s));
+    if (prof) SBWT_CHECK_CUDA(cudaEventRecord(ix->prof_ev[1], s));
+    SBWT_TRY(launch_kstart(d_rows, n_rows, ix->k, w.kstart, w.scan, s));
+    SBWT_TRY(launch_chunk_rows(w.kstart, n_rows, n_kmers, a.chunk, w.chunk_row, s));
+    if (prof) SBWT_CHECK_CUDA(cudaEventRecord(ix->prof_ev[2], s));
+    a.words = w.words;
+    a.positions = nullptr;
+    a.row_starts = d_rows;
+    a.kstart = w.kstart;
+    a.chunk_row = w.chunk_row;
+    a.n_rows = n_rows;
+    a.max_pos = (n_words - 1) * 32 - 1;
+    a.answers = d_answers;
+    a.n_kmers = n_kmers;
+    a.counter = w.counter;
+    uint32_t blocks = 0;
+    SBWT_TRY(launch_search(ix, a, s, &blocks));
+    if (prof) SBWT_CHECK_CUDA(cudaEventRecord(ix->prof_ev[3], s));
+    if (d_member) SBWT_TRY(launch_member_bits(d_answers, n_kmers, d_member, s));
+    if (prof) {
+        SBWT_CHECK_CUDA(cudaEventRecord(ix->prof_ev[4], s));
+        ix->prof_launches = 1 + 3 + 1 + 1 + (d_member ? 1 : 0);
+        ix->prof_blocks = blocks;
+        ix->prof_member = d_member != nullptr;
+    }
+    return 0;
+}
+
+}  // namespace sbwt
+
+extern "C" int sbwt_search_packed(sbwt_index *ix, const uint64_t *d_kmer_string, uint64_t n_words,
+                                  uint64_t *d_positions_in_results_out, uint64_t n_kmers, void *stream) {
+    clear_error();
+    if (!ix) return set_error("index is NULL");
+    if (n_kmers == 0) return 0;
+    if (!d_kmer_string || !d_positions_in_results_out) return set_error("NULL device pointer");
+    if (n_words < 2) return set_error("the packed k-mer string needs at least 2 words (one of padding)");
+    SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    Workspace &w = ix->ws[0];
+    SBWT_TRY(grow(w.counter, w.counter_cap, 1));
+    SearchArgs a = base_args(ix);
+    a.words = d_kmer_string;
+    a.positions = d_positions_in_results_out;
+    a.max_pos = (n_words - 1) * 32 - 1;
+    a.answers = d_positions_in_results_out;
+    a.n_kmers = n_kmers;
+    a.counter = w.counter;
+    return launch_search(ix, a, s, nullptr);
+}
+
+extern "C" int sbwt_pack(const uint8_t *d_letters, uint64_t n_letters, uint64_t *d_words, void *stream) {
+    clear_error();
+    if (!d_letters && n_letters) return set_error("NULL device pointer");
+    if (!d_words) return set_error("NULL device pointer");
+    return launch_pack(d_letters, n_letters, d_words, (cudaStream_t)stream);
+}
+
+extern "C" int sbwt_search_reads(sbwt_index *ix, const uint8_t *d_letters, uint64_t n_letters,
+                                 const uint64_t *d_row_starts, uint64_t n_rows, uint64_t *d_answers,
+                                 uint32_t *d_member_bits, uint64_t n_kmers, void *stream) {
+    clear_error();
+    if (!ix) return set_error("index is NULL");
+    if (n_rows && (!d_letters || !d_row_starts)) return set_error("NULL device pointer");
+    if (n_kmers && !d_answers) return set_error("NULL answers pointer");
+    SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
+    return search_rows_device(ix, ix->ws[0], d_letters, n_letters, d_row_starts, n_rows, d_answers, d_member_bits,
+                              n_kmers, (cudaStream_t)stream);
+}
+
+extern "C" int sbwt_profile_enable(sbwt_index *ix, int on) {
+    clear_error();
+    if (!ix) return set_error("index is NULL");
+    SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
+    if (on) {
+        for (auto &e : ix->prof_ev)
+            if (!e) SBWT_CHECK_CUDA(cudaEventCreate(&e));
+    }
+    ix->prof_on = on != 0;
+    ix->prof_launches = 0;
+    return 0;
+}
+
+extern "C" int sbwt_profile_read(sbwt_index *ix, sbwt_profile *out) {
+    clear_error();
+    if (!ix || !out) return set_error("NULL argument");
+    if (!ix->prof_on || ix->prof_launches == 0) return set_error("no profiled call (sbwt_profile_enable first)");
+    SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
+    SBWT_CHECK_CUDA(cudaEventSynchronize(ix->prof_ev[4]));
+    float t[4];
+    for (int i = 0; i < 4; i++) SBWT_CHECK_CUDA(cudaEventElapsedTime(&t[i], ix->prof_ev[i], ix->prof_ev[i + 1]));
+    out->pack_ms = t[0];
+    out->table_ms = t[1];
+    out->search_ms = t[2];
+    out->member_ms = ix->prof_member ? t[3] : 0.0f;
+    out->launches = ix->prof_launches;
+    out->search_blocks = ix->prof_blocks;
+    return 0;
+}
+
+extern "C" uint64_t sbwt_count_kmers(const uint64_t *row_starts, uint64_t n_rows, uint32_t k) {
+    uint64_t t = 0;
+    for (uint64_t r = 0; r < n_rows; r++) {
+        const uint64_t len = row_starts[r + 1] - row_starts[r];
+        if (len >= k) t += len - k + 1;
+    }
+    return t;
+}

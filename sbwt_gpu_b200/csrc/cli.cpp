@@ -1,0 +1,193 @@
+// cli.cpp -- `sbwt_search`, the command-line drop-in for the reference's
+// build/search program (src/search.cpp:9-26).  Flags keep the reference's
+// names and ranges (include/parameters.hpp:13-37, 79-297); answers go to
+// stdout in the reference's format (include/epicseq/results_persister.hpp:
+// 82-95), timings to stderr.
+//
+//   sbwt_search --file-a=A --file-c=C --file-g=G --file-t=T --file-queries=Q
+//               [--k=30] [--k-presearch=12] [--without-presearch]
+//               [--bits-in-superblock=1024] [--rank-structure=poppy|cum-poppy]
+//               [--with-shuffles] [--threads-per-block=N]
+//               [--device-set-limit-presearch=64] [--device-set-limit-search=64]
+//               [--do-not-store-results] [--layout=lines|poppy]
+//               [--kmers-per-thread=N] [--threads-per-kmer=1|2|4]
+//
+// Differences from the reference: errors return a non-zero exit status
+// (the reference always returns 0, src/search.cpp:14-25); --rank-structure=
+// flat-poppy, which the reference parses but never implements
+// (parameters.hpp:196-200), is rejected; --unified-searches and
+// --rank-word-size (unused on the reference's live path) are accepted and
+// ignored.
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <regex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "sbwt_gpu.h"
+
+namespace {
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void print_help() {
+    std::fprintf(stderr,
+                 "usage: sbwt_search --file-a=A --file-c=C --file-g=G --file-t=T --file-queries=Q [--k=30]\n"
+                 "       [--k-presearch=12 | --without-presearch] [--bits-in-superblock=1024]\n"
+                 "       [--rank-structure=poppy|cum-poppy] [--with-shuffles] [--threads-per-block=N]\n"
+                 "       [--device-set-limit-presearch=32|64|128] [--device-set-limit-search=32|64|128]\n"
+                 "       [--do-not-store-results] [--layout=lines|poppy] [--kmers-per-thread=N]\n"
+                 "       [--threads-per-kmer=1|2|4]\n");
+}
+
+struct Options {
+    std::string a, c, g, t, queries;
+    bool with_presearch = true, store = true;
+    int limit_presearch = 64, limit_search = 64;
+    sbwt_params p;
+};
+
+int parse(int argc, char **argv, Options &o) {
+    sbwt_params_default(&o.p);
+    if (argc == 1 || std::string(argv[1]) == "help") {
+        print_help();
+        return 2;
+    }
+    const std::regex sb_re{"^--bits-in-superblock=(256|512|1024|2048|4096)$"};
+    const std::regex lp_re{"^--device-set-limit-presearch=(32|64|128)$"};
+    const std::regex ls_re{"^--device-set-limit-search=(32|64|128)$"};
+    const std::regex k_re{"^--k=([3-9]|([1-2][0-9])|3[0-2])$"};
+    const std::regex kp_re{"^--k-presearch=([1-9]|(1[0-5]))$"};
+    const std::regex tpb_re{"^--threads-per-block=([0-9][0-9][0-9]?[0-9]?)$"};
+    const std::regex kpt_re{"^--kmers-per-thread=([1-8])$"};
+    const std::regex tpk_re{"^--threads-per-kmer=(1|2|4)$"};
+    std::smatch m;
+    for (int i = 1; i < argc; i++) {
+        const std::string s = argv[i];
+        auto val = [&](const char *prefix) { return s.substr(std::strlen(prefix)); };
+        if (s == "--without-presearch") o.with_presearch = false;
+        else if (s == "--do-not-store-results") o.store = false;
+        else if (s == "--with-shuffles") o.p.with_shuffles = 1;
+        else if (s == "--rank-structure=poppy") o.p.rank_structure = SBWT_POPPY;
+        else if (s == "--rank-structure=cum-poppy") o.p.rank_structure = SBWT_CUM_POPPY;
+        else if (s == "--rank-structure=flat-poppy") {
+            std::fprintf(stderr, "The rank structure flat-poppy has no implementation.\n");
+            return 1;
+        } else if (s == "--unified-searches" || s.rfind("--rank-word-size=", 0) == 0) {
+            std::fprintf(stderr, "Ignoring %s.\n", s.c_str());
+        } else if (s == "--layout=lines") o.p.layout = SBWT_LAYOUT_LINES;
+        else if (s == "--layout=poppy") o.p.layout = SBWT_LAYOUT_POPPY;
+        else if (std::regex_match(s, m, sb_re)) o.p.bits_in_superblock = (uint32_t)std::stoul(m[1]);
+        else if (std::regex_match(s, m, lp_re)) o.limit_presearch = std::stoi(m[1]);
+        else if (std::regex_match(s, m, ls_re)) o.limit_search = std::stoi(m[1]);
+        else if (std::regex_match(s, m, k_re)) o.p.k = (uint32_t)std::stoul(m[1]);
+        else if (std::regex_match(s, m, kp_re)) o.p.k_presearch = (uint32_t)std::stoul(m[1]);
+        else if (std::regex_match(s, m, kpt_re)) o.p.kmers_per_thread = (uint32_t)std::stoul(m[1]);
+        else if (std::regex_match(s, m, tpk_re)) o.p.threads_per_kmer = (uint32_t)std::stoul(m[1]);
+        else if (std::regex_match(s, m, tpb_re)) {
+            const unsigned v = (unsigned)std::stoul(m[1]);
+            if (v < 32 || v > 256 || v % 32)  // parameters.hpp:223-231 (our kernels take at most 256)
+                std::fprintf(stderr, "Number of threads per block should have been at least 32 and at most 256. "
+                                     "We use now the default.\n");
+            else
+                o.p.threads_per_block = v;
+        } else if (s.rfind("--file-a=", 0) == 0) o.a = val("--file-a=");
+        else if (s.rfind("--file-c=", 0) == 0) o.c = val("--file-c=");
+        else if (s.rfind("--file-g=", 0) == 0) o.g = val("--file-g=");
+        else if (s.rfind("--file-t=", 0) == 0) o.t = val("--file-t=");
+        else if (s.rfind("--file-queries=", 0) == 0) o.queries = val("--file-queries=");
+        else if (s.rfind("--file-answers=", 0) == 0) { /* the reference's legacy checker only */ }
+        else std::fprintf(stderr, "Unknown argument %s ignored.\n", s.c_str());
+    }
+    if (o.with_presearch) {
+        if (o.p.k_presearch < 5 || o.p.k_presearch > 13) {  // parameters.hpp:244-252
+            std::fprintf(stderr, "The value of the prefix of k-mers to be presearched must be at least 5 and at most 13.\n");
+            o.p.k_presearch = 12;
+        }
+        if (o.p.k_presearch > o.p.k) o.p.k_presearch = o.p.k;
+    } else {
+        o.p.k_presearch = 0;
+    }
+    if (o.p.bits_in_superblock == 4096 && o.p.rank_structure != SBWT_POPPY) {  // parameters.hpp:273-277
+        std::fprintf(stderr, "Superblock size 4096 bits is supported only in the rank structure version poppy. "
+                             "Please choose some other parameters.\n");
+        return 1;
+    }
+    if (o.a.empty() || o.c.empty() || o.g.empty() || o.t.empty() || o.queries.empty()) {
+        std::fprintf(stderr, "The four bit vector files and the query file are required.\n");
+        print_help();
+        return 1;
+    }
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+    Options o;
+    const int prc = parse(argc, argv, o);
+    if (prc == 2) return 0;
+    if (prc) return 1;
+    cudaSetDevice(o.p.device);
+    cudaDeviceSetLimit(cudaLimitMaxL2FetchGranularity, o.limit_presearch);  // presearch.hpp:34-37
+    auto t0 = std::chrono::steady_clock::now();
+    sbwt_index *ix = nullptr;
+    if (sbwt_index_load(o.a.c_str(), o.c.c_str(), o.g.c_str(), o.t.c_str(), &o.p, &ix)) {
+        std::fprintf(stderr, "%s\n", sbwt_last_error());
+        return 1;
+    }
+    uint64_t n = 0, C[5];
+    sbwt_index_info(ix, &n, C, nullptr, nullptr);
+    std::fprintf(stderr, "%f ms for reading the bit vector files, constructing the rank data structures, "
+                         "presearching and sending to the device (%llu columns).\n",
+                 ms_since(t0), (unsigned long long)n);
+    if (o.p.layout == SBWT_LAYOUT_POPPY &&
+        sbwt_configure(ix, SBWT_LAYOUT_POPPY, o.p.bits_in_superblock, o.p.rank_structure, o.p.with_shuffles,
+                       o.p.kmers_per_thread, o.p.threads_per_kmer, o.p.threads_per_block)) {
+        std::fprintf(stderr, "%s\n", sbwt_last_error());
+        sbwt_index_free(ix);
+        return 1;
+    }
+    cudaDeviceSetLimit(cudaLimitMaxL2FetchGranularity, o.limit_search);  // search_caller.hpp:91-96
+    auto t1 = std::chrono::steady_clock::now();
+    sbwt_queries q;
+    if (sbwt_queries_read(o.queries.c_str(), o.p.k, &q)) {
+        std::fprintf(stderr, "%s\n", sbwt_last_error());
+        sbwt_index_free(ix);
+        return 1;
+    }
+    const double ms_read = ms_since(t1);
+    std::vector<uint64_t> answers(q.n_kmers ? q.n_kmers : 1);
+    auto t2 = std::chrono::steady_clock::now();
+    if (sbwt_search_reads_host(ix, q.letters, q.n_letters, q.row_starts, q.n_rows, answers.data(), q.n_kmers)) {
+        std::fprintf(stderr, "%s\n", sbwt_last_error());
+        sbwt_queries_free(&q);
+        sbwt_index_free(ix);
+        return 1;
+    }
+    const double ms_search = ms_since(t2);
+    std::fprintf(stderr, "Reading the query file: %f ms.\n", ms_read);
+    std::fprintf(stderr, "Search (host to device, pack, search, device to host): %f ms.\n", ms_search);
+    std::fprintf(stderr, "Number of k-mers queried: %llu\n", (unsigned long long)q.n_kmers);
+    if (q.n_kmers)
+        std::fprintf(stderr, "Total per query: %f ns.\n", ms_search * 1e6 / (double)q.n_kmers);
+    int rc = 0;
+    if (o.store) {
+        const int64_t bytes = sbwt_format_answers(q.row_starts, q.n_rows, o.p.k, answers.data(), nullptr, 0);
+        std::vector<char> text((size_t)bytes + 1);
+        sbwt_format_answers(q.row_starts, q.n_rows, o.p.k, answers.data(), text.data(), (uint64_t)text.size());
+        if (std::fwrite(text.data(), 1, (size_t)bytes, stdout) != (size_t)bytes) rc = 1;
+        std::fflush(stdout);
+    } else {
+        std::fprintf(stderr, "The results are not stored to the file.\n");
+    }
+    sbwt_queries_free(&q);
+    sbwt_index_free(ix);
+    return rc;
+}

@@ -1,0 +1,137 @@
+// device.cuh -- device-side layouts and rank functions (sm_100a).
+//
+// Two rank layouts are served:
+//
+//  * LINES (this engine's search layout).  Each of the four vectors is cut
+//    into 224-bit blocks; block b is stored as one 32-byte line (= one L2
+//    sector) holding a 32-bit count of the ones before the block followed by
+//    the block's 224 bits.  Line bits are MSB-first across the four u64
+//    words: word0 = count << 32 | bits 0..31, word1 = bits 32..95,
+//    word2 = bits 96..159, word3 = bits 160..223 (bit q of the block at line
+//    bit 32+q, line bit b at bit 63-b%64 of word b/64).  rank_c(i) is one
+//    256-bit load plus a masked popcount: one sector per rank, where the
+//    reference's poppy needs an L12 word and a basic block in different
+//    sectors (include/gpu/rank_kernel.hpp:212-296).  Counts are 32-bit, so
+//    the layout serves indexes of fewer than 224 * 2^24 - 1 columns.
+//
+//  * POPPY (the reference layout).  L0 / L12 words exactly as
+//    RankDataStructures builds them (include/rank_data_structures.hpp:
+//    142-198) over the raw vectors; rank as include/gpu/rank_kernel.hpp:
+//    212-296 + 409-415 defines it.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sbwt {
+namespace dev {
+
+using u64 = uint64_t;
+using u32 = uint32_t;
+
+constexpr u32 kLineBits = 224;      // data bits per 32-byte line
+constexpr u32 kLineBytes = 32;
+constexpr u32 kMaxLinesPerChar = 1u << 24;  // 32-bit counts: 224 * 2^24 < 2^32
+
+// 256-bit read-only load of one line (sm_100 supports .v4.u64 global loads).
+__device__ __forceinline__ ulonglong4 ld_line(const ulonglong4 *p) {
+    ulonglong4 v;
+    asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];"
+        : "=l"(v.x), "=l"(v.y), "=l"(v.z), "=l"(v.w)
+        : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ ulonglong2 ld_nc2(const ulonglong2 *p) {
+    ulonglong2 v;
+    asm("ld.global.nc.v2.u64 {%0, %1}, [%2];" : "=l"(v.x), "=l"(v.y) : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ u64 ld_nc(const u64 *p) {
+    u64 v;
+    asm("ld.global.nc.u64 %0, [%1];" : "=l"(v) : "l"(p));
+    return v;
+}
+
+// x >> s with the PTX rule that s >= 64 gives 0 (the reference relies on it,
+// include/gpu/rank_kernel.hpp:218,226-229).
+__device__ __forceinline__ u64 shr_clamp(u64 x, u32 s) {
+    u64 r;
+    asm("shr.b64 %0, %1, %2;" : "=l"(r) : "l"(x), "r"(s));
+    return r;
+}
+
+__device__ __forceinline__ u32 shr_clamp32(u32 x, u32 s) {
+    u32 r;
+    asm("shr.b32 %0, %1, %2;" : "=r"(r) : "r"(x), "r"(s));
+    return r;
+}
+
+// Ones among the top `b` bits of w, b in [0, 64].
+__device__ __forceinline__ u32 popc_top(u64 w, u32 b) { return __popcll(shr_clamp(w, 64u - b)); }
+
+__device__ __forceinline__ u32 clamp64(int v) { return (u32)min(max(v, 0), 64); }
+
+// Ones among the first q data bits of a line (q in [0, 224]).
+__device__ __forceinline__ u32 line_prefix(const ulonglong4 &w, u32 q) {
+    const int t = (int)q + 32;  // line bits [32, t)
+    return popc_top(w.x & 0xffffffffull, clamp64(t)) + popc_top(w.y, clamp64(t - 64)) +
+           popc_top(w.z, clamp64(t - 128)) + popc_top(w.w, clamp64(t - 192));
+}
+
+// Partial form used when TPK lanes share a line: lane `part` of `parts`
+// (parts = 2: two u64 words each; parts = 4: one word each) counts its words.
+__device__ __forceinline__ u32 word_prefix(u64 w, u32 word_index, u32 q) {
+    const int t = (int)q + 32 - 64 * (int)word_index;
+    if (word_index == 0) w &= 0xffffffffull;
+    return popc_top(w, clamp64(t));
+}
+
+// rank of line layout: count stored in the line + prefix popcount.
+__device__ __forceinline__ u32 line_rank_from(const ulonglong4 &w, u32 q) {
+    return (u32)(w.x >> 32) + line_prefix(w, q);
+}
+
+__device__ __forceinline__ void line_split(u32 x, u32 &line, u32 &q) {
+    line = x / kLineBits;
+    q = x - line * kLineBits;
+}
+
+// ------------------------------------------------------------------ poppy
+
+template <int SB> struct PoppyShape {
+    static constexpr int kLogSB = SB == 256 ? 8 : SB == 512 ? 9 : SB == 1024 ? 10 : SB == 2048 ? 11 : 12;
+    static constexpr int kLogBB = kLogSB - 2;
+    static constexpr int kWordsBB = SB / 256;             // u64 words per basic block
+    static constexpr int kLogHyper = SB == 4096 ? 31 : 32;  // rank_data_structures.hpp:64-66
+    static constexpr int kRelShift = SB == 4096 ? 33 : 32;
+};
+
+// Ones of the basic blocks of superblock entry e that precede basic block b
+// (include/gpu/rank_kernel.hpp:253-296).
+template <int SB, int KIND>
+__device__ __forceinline__ u64 poppy_before_bb(u64 e, u32 b) {
+    if (KIND == 1) {
+        if (SB == 4096) {
+            const u64 bc = shr_clamp(e & 0x1ffffffffull, (3u - b) * 11u);
+            return (e >> 33) + ((bc & 0x7ffu) + ((bc >> 11) & 0x7ffu) + (bc >> 22));
+        }
+        const u32 bc = shr_clamp32((u32)(e & 0x3fffffffu), (3u - b) * 10u);
+        return (e >> 32) + ((bc & 0x3ffu) + ((bc >> 10) & 0x3ffu) + ((bc >> 20) & 0x3ffu));
+    }
+    if (SB == 2048) {
+        const u32 bc = shr_clamp32((u32)(e & 0xffffffffu), (3u - b) * 11u);
+        return (e >> 32) + (bc & 0x7ffu);
+    }
+    const u32 bc = shr_clamp32((u32)(e & 0x3fffffffu), (3u - b) * 10u);
+    return (e >> 32) + (bc & 0x3ffu);
+}
+
+// Ones of word j of a basic block that precede position i (word iw holds i).
+__device__ __forceinline__ u32 bb_word_prefix(u64 w, u32 j, u32 iw, u32 i63) {
+    const u32 s = (j == iw) ? (64u - i63) : (j > iw ? 64u : 0u);
+    return __popcll(shr_clamp(w, s));
+}
+
+}  // namespace dev
+}  // namespace sbwt

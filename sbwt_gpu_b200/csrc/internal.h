@@ -1,0 +1,142 @@
+// internal.h -- the index handle and the host-side launchers shared by the
+// CUDA translation units.  Not part of the C ABI.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sbwt_gpu.h"
+#include "common.h"
+
+namespace sbwt {
+
+using u64 = uint64_t;
+using u32 = uint32_t;
+
+// Device-side parameters of one search launch (passed by value).
+struct SearchArgs {
+    // LINES layout
+    const ulonglong4 *lines;
+    u32 lpc;  // lines per vector
+    // POPPY layout
+    const u64 *bits;  // 4 vectors of wpv words
+    const u64 *L0;    // 4 x l0w words
+    const u64 *L12;   // 4 x l12w words
+    u64 wpv, l0w, l12w;
+    // common
+    u64 C[5];
+    const void *pre;  // presearch table: uint2 (n < 2^32) or ulonglong2 entries; NULL if p == 0
+    u32 p;
+    u32 k;
+    const u64 *words;       // packed letters
+    const u64 *positions;   // reference contract: letter offset of k-mer j (NULL: read mode)
+    const u64 *row_starts;  // read mode: letter offset of each row (n_rows + 1)
+    const u64 *kstart;      // read mode: first k-mer index of each row (n_rows + 1)
+    const u32 *chunk_row;   // read mode: row of the first k-mer of each chunk
+    u64 n_rows;             // read mode: rows (kstart[n_rows] = k-mers in the batch)
+    u64 max_pos;            // largest letter offset whose 64-bit window lies inside `words`
+    u64 *answers;
+    u64 n_kmers;
+    unsigned long long *counter;  // work-stealing cursor (zeroed before launch)
+    u32 chunk;                    // k-mers per grab
+};
+
+struct KernelShape {
+    int layout = SBWT_LAYOUT_LINES;
+    u32 kpt = 2;   // k-mer slots per thread
+    u32 tpk = 1;   // lanes per k-mer
+    u32 tpb = 256; // threads per block
+    u32 sb = 1024;
+    int kind = SBWT_POPPY;
+    int shuffles = 0;
+};
+
+// Device buffers of one in-flight search (grow-only).
+struct Workspace {
+    uint64_t *words = nullptr;  size_t words_cap = 0;
+    uint64_t *kstart = nullptr; size_t kstart_cap = 0;
+    uint32_t *chunk_row = nullptr; size_t chunk_cap = 0;
+    uint64_t *scan = nullptr;   size_t scan_cap = 0;
+    unsigned long long *counter = nullptr; size_t counter_cap = 0;
+    // host pipeline only
+    uint8_t *letters = nullptr; size_t letters_cap = 0;
+    uint64_t *rows = nullptr;   size_t rows_cap = 0;
+    uint64_t *answers = nullptr; size_t answers_cap = 0;
+    uint64_t *h_rows = nullptr; size_t h_rows_cap = 0;  // pinned host staging
+    uint8_t *h_letters = nullptr; size_t h_letters_cap = 0;
+    uint64_t *h_answers = nullptr; size_t h_answers_cap = 0;
+    void release();
+};
+
+}  // namespace sbwt
+
+struct sbwt_index {
+    int device = 0;
+    int num_sms = 0;
+    uint64_t n = 0;
+    uint32_t k = 30;
+    uint64_t C[5] = {0, 0, 0, 0, 0};
+    // raw vectors (reference word layout), 4 x wpv words, zero past n
+    uint64_t *d_bits = nullptr;
+    uint64_t wpv = 0;
+    // LINES layout
+    ulonglong4 *d_lines = nullptr;
+    uint32_t lpc = 0;
+    bool lines_ok = false;
+    // POPPY layout
+    uint64_t *d_L0 = nullptr, *d_L12 = nullptr;
+    uint64_t l0w = 0, l12w = 0;
+    uint32_t sb = 0;
+    int kind = 0;
+    bool poppy_ok = false;
+    // presearch table
+    uint32_t p = 0;
+    void *d_pre = nullptr;
+    bool pre64 = false;
+    // launch shape
+    sbwt::KernelShape shape;
+    // scan block sums of the rank builds
+    uint64_t *d_scan = nullptr;
+    size_t scan_cap = 0;
+    // per-call work buffers: ws[0] serves the device-pointer entry points,
+    // ws[0] and ws[1] the two streams of the host pipeline
+    sbwt::Workspace ws[2];
+    cudaStream_t pipe_stream[2] = {nullptr, nullptr};
+    // per-call profiling (sbwt_profile_enable)
+    bool prof_on = false;
+    cudaEvent_t prof_ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    uint32_t prof_launches = 0, prof_blocks = 0;
+    bool prof_member = false;
+};
+
+namespace sbwt {
+
+// rank_build.cu
+int build_lines(sbwt_index *ix, cudaStream_t s, uint64_t ones[4]);
+int build_poppy(sbwt_index *ix, uint32_t sb, int kind, cudaStream_t s);
+int ensure_scan_scratch(sbwt_index *ix, uint64_t n_items);
+
+// presearch.cu
+int run_presearch(sbwt_index *ix, uint32_t p, cudaStream_t s);
+int export_presearch(const sbwt_index *ix, uint64_t *lefts, uint64_t *rights, uint64_t count);
+
+// ingest.cu
+int launch_pack(const uint8_t *d_letters, uint64_t n_letters, uint64_t *d_words, cudaStream_t s);
+int launch_kstart(const uint64_t *d_row_starts, uint64_t n_rows, uint32_t k, uint64_t *d_kstart, uint64_t *d_scan,
+                  cudaStream_t s);
+uint64_t scan_scratch_words(uint64_t n_items);
+int launch_chunk_rows(const uint64_t *d_kstart, uint64_t n_rows, uint64_t n_kmers, uint32_t chunk,
+                      uint32_t *d_chunk_row, cudaStream_t s);
+int launch_member_bits(const uint64_t *d_answers, uint64_t n, uint32_t *d_bits, cudaStream_t s);
+
+// api.cu
+int search_rows_device(sbwt_index *ix, Workspace &w, const uint8_t *d_letters, u64 n_letters, const u64 *d_rows,
+                       u64 n_rows, u64 *d_answers, uint32_t *d_member, u64 n_kmers, cudaStream_t s);
+template <class T> int grow(T *&p, size_t &cap, size_t need);
+template <class T> int grow_host(T *&p, size_t &cap, size_t need);
+
+// search.cu
+int launch_search(const sbwt_index *ix, SearchArgs &a, cudaStream_t s, uint32_t *launched_blocks);
+u32 search_chunk(const KernelShape &sh);
+bool search_shape_supported(const KernelShape &sh, bool wide);
+
+}  // namespace sbwt

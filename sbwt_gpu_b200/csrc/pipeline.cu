@@ -1,0 +1,136 @@
+// pipeline.cu -- sbwt_search_reads_host: a batch of reads in host memory is
+// streamed through the GPU in chunks of rows.  Two CUDA streams alternate;
+// on each, a chunk's letters and row table go host->device, the chunk is
+// packed and searched, and its answers come back device->host, so the copies
+// of one chunk overlap the search of the other.
+//
+// This replaces the strictly sequential host<->device chain of the reference
+// (KmerSearch::search, include/epicseq/kmer_search.hpp:97-160: one H2D of the
+// whole query, pack, positions, search, then one D2H of all results in
+// ResultsPersister::save_results_to_file, results_persister.hpp:58-65).
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "internal.h"
+
+namespace sbwt {
+namespace {
+
+bool is_pinned(const void *p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
+struct Chunk {
+    u64 r0, r1;  // rows [r0, r1)
+    u64 l0, l1;  // letters [l0, l1)
+    u64 k0, nk;  // answers [k0, k0 + nk)
+};
+
+// Letters per chunk: large enough to amortise the launches, small enough
+// that two chunks in flight stay well inside device memory.
+constexpr u64 kChunkLetters = 64ull << 20;
+
+}  // namespace
+}  // namespace sbwt
+
+using namespace sbwt;
+
+extern "C" int sbwt_search_reads_host(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters,
+                                      const uint64_t *row_starts, uint64_t n_rows, uint64_t *answers,
+                                      uint64_t n_kmers) {
+    clear_error();
+    if (!ix) return set_error("index is NULL");
+    if (n_rows == 0) return 0;
+    if (!letters || !row_starts || (n_kmers && !answers)) return set_error("NULL host pointer");
+    if (row_starts[n_rows] > n_letters) return set_error("row_starts[n_rows] exceeds n_letters");
+    for (u64 r = 0; r < n_rows; r++)
+        if (row_starts[r + 1] < row_starts[r]) return set_error("row_starts must be non-decreasing (row %llu)",
+                                                                (unsigned long long)r);
+    const u32 k = ix->k;
+    // chunks of whole rows
+    std::vector<Chunk> chunks;
+    {
+        Chunk c{0, 0, row_starts[0], row_starts[0], 0, 0};
+        u64 kk = 0;
+        for (u64 r = 0; r < n_rows; r++) {
+            const u64 len = row_starts[r + 1] - row_starts[r];
+            const u64 nk = len >= k ? len - k + 1 : 0;
+            c.r1 = r + 1;
+            c.l1 = row_starts[r + 1];
+            c.nk += nk;
+            kk += nk;
+            if (c.l1 - c.l0 >= kChunkLetters || r + 1 == n_rows) {
+                chunks.push_back(c);
+                c = Chunk{r + 1, r + 1, row_starts[r + 1], row_starts[r + 1], kk, 0};
+            }
+        }
+        if (kk != n_kmers)
+            return set_error("n_kmers = %llu but the rows hold %llu k-mers", (unsigned long long)n_kmers,
+                             (unsigned long long)kk);
+    }
+    SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
+    for (int i = 0; i < 2; i++)
+        if (!ix->pipe_stream[i]) SBWT_CHECK_CUDA(cudaStreamCreateWithFlags(&ix->pipe_stream[i], cudaStreamNonBlocking));
+    const bool pin_in = is_pinned(letters);
+    const bool pin_out = n_kmers == 0 || is_pinned(answers);
+    u64 max_letters = 0, max_rows = 0, max_k = 0;
+    for (const Chunk &c : chunks) {
+        max_letters = std::max(max_letters, c.l1 - c.l0);
+        max_rows = std::max(max_rows, c.r1 - c.r0);
+        max_k = std::max(max_k, c.nk);
+    }
+    for (int i = 0; i < 2; i++) {
+        Workspace &w = ix->ws[i];
+        SBWT_TRY(grow(w.letters, w.letters_cap, max_letters + 16));
+        SBWT_TRY(grow(w.rows, w.rows_cap, max_rows + 1));
+        SBWT_TRY(grow(w.answers, w.answers_cap, max_k));
+        SBWT_TRY(grow_host(w.h_rows, w.h_rows_cap, max_rows + 1));
+        if (!pin_in) SBWT_TRY(grow_host(w.h_letters, w.h_letters_cap, max_letters + 16));
+        if (!pin_out) SBWT_TRY(grow_host(w.h_answers, w.h_answers_cap, max_k));
+    }
+    // pending[i]: chunk whose answers sit in slot i's pinned staging (pageable output)
+    long pending[2] = {-1, -1};
+    auto drain = [&](int slot) -> int {
+        SBWT_CHECK_CUDA(cudaStreamSynchronize(ix->pipe_stream[slot]));
+        if (pending[slot] >= 0) {
+            const Chunk &c = chunks[(size_t)pending[slot]];
+            std::memcpy(answers + c.k0, ix->ws[slot].h_answers, c.nk * sizeof(u64));
+            pending[slot] = -1;
+        }
+        return 0;
+    };
+    for (size_t b = 0; b < chunks.size(); b++) {
+        const int slot = (int)(b & 1);
+        const Chunk &c = chunks[b];
+        cudaStream_t s = ix->pipe_stream[slot];
+        Workspace &w = ix->ws[slot];
+        SBWT_TRY(drain(slot));  // slot's previous chunk has finished with its buffers
+        const u64 nr = c.r1 - c.r0, nl = c.l1 - c.l0;
+        for (u64 r = 0; r <= nr; r++) w.h_rows[r] = row_starts[c.r0 + r] - c.l0;
+        SBWT_CHECK_CUDA(cudaMemcpyAsync(w.rows, w.h_rows, (nr + 1) * sizeof(u64), cudaMemcpyHostToDevice, s));
+        if (pin_in) {
+            SBWT_CHECK_CUDA(cudaMemcpyAsync(w.letters, letters + c.l0, nl, cudaMemcpyHostToDevice, s));
+        } else {
+            std::memcpy(w.h_letters, letters + c.l0, nl);
+            SBWT_CHECK_CUDA(cudaMemcpyAsync(w.letters, w.h_letters, nl, cudaMemcpyHostToDevice, s));
+        }
+        SBWT_TRY(search_rows_device(ix, w, w.letters, nl, w.rows, nr, w.answers, nullptr, c.nk, s));
+        if (c.nk) {
+            if (pin_out) {
+                SBWT_CHECK_CUDA(cudaMemcpyAsync(answers + c.k0, w.answers, c.nk * sizeof(u64), cudaMemcpyDeviceToHost, s));
+            } else {
+                SBWT_CHECK_CUDA(cudaMemcpyAsync(w.h_answers, w.answers, c.nk * sizeof(u64), cudaMemcpyDeviceToHost, s));
+                pending[slot] = (long)b;
+            }
+        }
+    }
+    SBWT_TRY(drain(0));
+    SBWT_TRY(drain(1));
+    return 0;
+}

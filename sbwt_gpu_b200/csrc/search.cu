@@ -1,0 +1,244 @@
+// search.cu -- the per-k-mer SBWT search (the hot path).
+//
+// Replaces epic::gpu::search (include/gpu/search_kernel.hpp:61-104), launched
+// one thread per k-mer by launch_search_kernel (include/gpu/
+// search_and_presearch_launchers.hpp:21-60), together with the per-read
+// positions kernel (include/gpu/positions_kernel.hpp:18-36).
+//
+// Semantics kept from the reference, per k-mer:
+//   kmer  = 64 bits from letter offset pos (search_kernel.hpp:66-68)
+//   [l,r] = presearch entry of its first p letters, or [0, C[4]-1] without
+//           presearch (:71-82)
+//   for i = p..k-1: one rank-pair step with letter i, stop once l > r (:84-96)
+//   answer = l if l <= r else 0xFFFF_FFFF_FFFF_FFFF (:98-103)
+// An interval that is already empty is not stepped (an empty interval stays
+// empty, so the answer is the same).
+//
+// Launch shape (this engine's own): a persistent grid of (#SMs x resident
+// blocks).  Each warp takes chunks of consecutive k-mer indices from a global
+// atomic cursor (work stealing), and each lane keeps KPT k-mers in flight in
+// registers; a lane whose k-mer finishes takes the next index of its warp's
+// chunk at once (ballot + popc), so lanes never idle behind a long k-mer.
+// With TPK > 1, TPK lanes share one k-mer and split every 32-byte line.
+// K-mers are located either through the reference's positions array
+// (sbwt_search_packed) or through a per-row table (sbwt_search_reads): no
+// positions array is materialised there.
+#include <algorithm>
+
+#include "device.cuh"
+#include "internal.h"
+#include "rank.cuh"
+
+namespace sbwt {
+namespace {
+
+using namespace dev;
+
+constexpr u32 kFull = 0xffffffffu;
+constexpr u32 kDone = 0xffffffffu;
+
+template <class IT> struct PairOf;
+template <> struct PairOf<u32> { using T = uint2; };
+template <> struct PairOf<u64> { using T = ulonglong2; };
+
+template <class R, int KPT, int TPK>
+__global__ void __launch_bounds__(256) search_kernel(const R rk, const SearchArgs a) {
+    using IT = typename R::IT;
+    using PT = typename PairOf<IT>::T;
+    const u32 lane = threadIdx.x & 31u;
+    const u32 sub = lane & (u32)(TPK - 1);
+    const u32 lead = lane - sub;
+    const u32 lead_lt = (1u << lead) - 1u;
+    const u32 gmask = TPK == 1 ? kFull : (((1u << TPK) - 1u) << lead);
+    const u32 k = a.k, p = a.p;
+    const IT C0 = (IT)a.C[0], C1 = (IT)a.C[1], C2 = (IT)a.C[2], C3 = (IT)a.C[3];
+    const IT rootR = (IT)(a.C[4] - 1ull);
+    const PT *pre = reinterpret_cast<const PT *>(a.pre);
+
+    u64 kmer[KPT], J[KPT];
+    IT L[KPT], R_[KPT];
+    u32 I[KPT];
+#pragma unroll
+    for (int s = 0; s < KPT; s++) { I[s] = kDone; kmer[s] = 0; J[s] = 0; L[s] = 0; R_[s] = 0; }
+
+    // k-mers of this launch; in read mode never more than the row table holds
+    const u64 n_eff = a.positions ? a.n_kmers : min(a.n_kmers, a.kstart[a.n_rows]);
+    u64 q_next = 0, q_end = 0, row = 0;
+    bool more = true;
+
+    for (;;) {
+        // ---- refill empty slots from the warp's chunk (work stealing)
+#pragma unroll
+        for (int s = 0; s < KPT; s++) {
+            while (more) {
+                const bool need = I[s] == kDone;
+                const u32 m = __ballot_sync(kFull, need && sub == 0);
+                if (m == 0) break;
+                if (q_next >= q_end) {
+                    unsigned long long base = 0;
+                    if (lane == 0) base = atomicAdd(a.counter, (unsigned long long)a.chunk);
+                    base = __shfl_sync(kFull, base, 0);
+                    if (base >= n_eff) { more = false; break; }
+                    q_next = base;
+                    q_end = min((u64)base + a.chunk, n_eff);
+                    if (!a.positions) row = a.chunk_row[base / a.chunk];
+                }
+                const u32 take = (u32)min((u64)__popc(m), q_end - q_next);
+                const u32 rk_ = __popc(m & lead_lt);
+                const bool got = need && rk_ < take;
+                u64 rr = row;
+                if (got) {
+                    const u64 j = q_next + rk_;
+                    u64 pos;
+                    if (a.positions) {
+                        pos = a.positions[j];
+                    } else {
+                        while (rr + 1 < a.n_rows && a.kstart[rr + 1] <= j) rr++;
+                        pos = a.row_starts[rr] + (j - a.kstart[rr]);
+                    }
+                    pos = min(pos, a.max_pos);  // a bad offset reads garbage, never out of bounds
+                    const u64 b = pos << 1;  // search_kernel.hpp:66-68
+                    const u64 w0 = a.words[b >> 6], w1 = a.words[(b >> 6) + 1];
+                    const u32 sh = (u32)(b & 63u);
+                    const u64 km = (w0 << sh) | (shr_clamp(w1, 63u - sh) >> 1);
+                    kmer[s] = km;
+                    J[s] = j;
+                    if (p) {
+                        const PT e = pre[km >> (64u - 2u * p)];
+                        L[s] = e.x;
+                        R_[s] = e.y;
+                    } else {
+                        L[s] = 0;
+                        R_[s] = rootR;
+                    }
+                    I[s] = p;
+                }
+                if (!a.positions) {
+                    const u32 lastm = __ballot_sync(kFull, got && sub == 0 && rk_ == take - 1u);
+                    row = __shfl_sync(kFull, rr, __ffs(lastm) - 1);
+                }
+                q_next += take;
+            }
+        }
+        bool act = false;
+#pragma unroll
+        for (int s = 0; s < KPT; s++) act |= I[s] != kDone;
+        if (!__any_sync(kFull, act)) break;
+
+        // ---- fetch: issue the loads of every stepping slot
+        typename R::Fetch F[KPT];
+        u32 cc[KPT];
+#pragma unroll
+        for (int s = 0; s < KPT; s++) {
+            cc[s] = 0;
+            if (I[s] < k && L[s] <= R_[s]) {
+                cc[s] = (u32)((kmer[s] >> (62u - 2u * I[s])) & 3u);
+                F[s] = rk.fetch(cc[s], L[s], R_[s], sub);
+            }
+        }
+        // ---- finish: popcounts, interval update, answers
+#pragma unroll
+        for (int s = 0; s < KPT; s++) {
+            if (I[s] < k && L[s] <= R_[s]) {
+                const u32 c = cc[s];
+                const IT Cc = c == 0 ? C0 : c == 1 ? C1 : c == 2 ? C2 : C3;
+                rk.finish(F[s], Cc, L[s], R_[s], sub, gmask);
+                I[s]++;
+            }
+            if (I[s] != kDone && (L[s] > R_[s] || I[s] >= k)) {
+                if (sub == 0) a.answers[J[s]] = (L[s] <= R_[s]) ? (u64)L[s] : ~0ull;
+                I[s] = kDone;
+            }
+        }
+    }
+}
+
+// -------------------------------------------------------------- dispatch
+
+template <class R, int KPT, int TPK>
+int launch_one(const R &rk, SearchArgs &a, const sbwt_index *ix, cudaStream_t s, u32 tpb, u32 *blocks_out) {
+    auto kern = search_kernel<R, KPT, TPK>;
+    int per_sm = 0;
+    SBWT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int)tpb, 0));
+    if (per_sm < 1) per_sm = 1;
+    const u32 blocks = (u32)per_sm * (u32)ix->num_sms;
+    if (blocks_out) *blocks_out = blocks;
+    SBWT_CHECK_CUDA(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), s));
+    kern<<<blocks, tpb, 0, s>>>(rk, a);
+    SBWT_CHECK_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template <int TPK>
+int lines_kpt(const sbwt_index *ix, SearchArgs &a, cudaStream_t s, u32 kpt, u32 tpb, u32 *blocks) {
+    LinesRankerT<TPK> rk{ix->d_lines, ix->lpc};
+    switch (kpt) {
+    case 1: return launch_one<LinesRankerT<TPK>, 1, TPK>(rk, a, ix, s, tpb, blocks);
+    case 2: return launch_one<LinesRankerT<TPK>, 2, TPK>(rk, a, ix, s, tpb, blocks);
+    case 3: return launch_one<LinesRankerT<TPK>, 3, TPK>(rk, a, ix, s, tpb, blocks);
+    case 4: return launch_one<LinesRankerT<TPK>, 4, TPK>(rk, a, ix, s, tpb, blocks);
+    case 6: return launch_one<LinesRankerT<TPK>, 6, TPK>(rk, a, ix, s, tpb, blocks);
+    case 8: return launch_one<LinesRankerT<TPK>, 8, TPK>(rk, a, ix, s, tpb, blocks);
+    default: return set_error("kmers_per_thread must be 1, 2, 3, 4, 6 or 8 (got %u)", kpt);
+    }
+}
+
+template <int SB, int KIND, class IT, int TPK>
+int poppy_kpt(const sbwt_index *ix, SearchArgs &a, cudaStream_t s, u32 kpt, u32 tpb, u32 *blocks) {
+    PoppyRanker<SB, KIND, IT, TPK> rk{ix->d_bits, ix->d_L0, ix->d_L12, ix->wpv, ix->l0w, ix->l12w};
+    using R = PoppyRanker<SB, KIND, IT, TPK>;
+    if (kpt >= 2 && sizeof(IT) == 4) return launch_one<R, 2, TPK>(rk, a, ix, s, tpb, blocks);
+    return launch_one<R, 1, TPK>(rk, a, ix, s, tpb, blocks);
+}
+
+template <int SB, int KIND>
+int poppy_sb(const sbwt_index *ix, SearchArgs &a, cudaStream_t s, const KernelShape &sh, u32 *blocks) {
+    const bool wide = ix->n >= (1ull << 32);
+    if (wide) return poppy_kpt<SB, KIND, u64, 1>(ix, a, s, 1, sh.tpb, blocks);
+    // the reference's shuffle variants exist for SB 1024 (2 lanes) and 2048 (4 lanes),
+    // include/gpu/rank_kernel.hpp:298-407
+    if (sh.shuffles && SB == 1024) return poppy_kpt<SB, KIND, u32, 2>(ix, a, s, sh.kpt, sh.tpb, blocks);
+    if (sh.shuffles && SB == 2048) return poppy_kpt<SB, KIND, u32, 4>(ix, a, s, sh.kpt, sh.tpb, blocks);
+    return poppy_kpt<SB, KIND, u32, 1>(ix, a, s, sh.kpt, sh.tpb, blocks);
+}
+
+}  // namespace
+
+u32 search_chunk(const KernelShape &sh) {
+    const u32 groups = 32u / (sh.layout == SBWT_LAYOUT_LINES ? sh.tpk : 1u);
+    return groups * std::max(sh.kpt, 1u) * 8u;
+}
+
+int launch_search(const sbwt_index *ix, SearchArgs &a, cudaStream_t s, uint32_t *blocks) {
+    const KernelShape &sh = ix->shape;
+    if (a.n_kmers == 0) return 0;
+    if (sh.tpb == 0 || sh.tpb % 32 != 0 || sh.tpb > 256)
+        return set_error("threads_per_block must be a multiple of 32 in [32, 256] (got %u)", sh.tpb);
+    if (sh.layout == SBWT_LAYOUT_LINES) {
+        if (!ix->lines_ok) return set_error("the line layout is not available for this index");
+        switch (sh.tpk) {
+        case 1: return lines_kpt<1>(ix, a, s, sh.kpt, sh.tpb, blocks);
+        case 2: return lines_kpt<2>(ix, a, s, sh.kpt, sh.tpb, blocks);
+        case 4: return lines_kpt<4>(ix, a, s, sh.kpt, sh.tpb, blocks);
+        default: return set_error("threads_per_kmer must be 1, 2 or 4 (got %u)", sh.tpk);
+        }
+    }
+    if (!ix->poppy_ok) return set_error("the poppy layout has not been built");
+    if (ix->kind == SBWT_POPPY) {
+        switch (ix->sb) {
+        case 256: return poppy_sb<256, 1>(ix, a, s, sh, blocks);
+        case 512: return poppy_sb<512, 1>(ix, a, s, sh, blocks);
+        case 1024: return poppy_sb<1024, 1>(ix, a, s, sh, blocks);
+        case 2048: return poppy_sb<2048, 1>(ix, a, s, sh, blocks);
+        default: return poppy_sb<4096, 1>(ix, a, s, sh, blocks);
+        }
+    }
+    switch (ix->sb) {
+    case 256: return poppy_sb<256, 2>(ix, a, s, sh, blocks);
+    case 512: return poppy_sb<512, 2>(ix, a, s, sh, blocks);
+    case 1024: return poppy_sb<1024, 2>(ix, a, s, sh, blocks);
+    default: return poppy_sb<2048, 2>(ix, a, s, sh, blocks);
+    }
+}
+
+}  // namespace sbwt

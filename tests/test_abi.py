@@ -1,0 +1,93 @@
+"""The C ABI without a GPU: the library loads, exports every declared symbol,
+and the host-side entry points behave like the reference's host code."""
+import os
+import re
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as orc
+import sbwt_gpu_b200 as sg
+from sbwt_gpu_b200 import _lib, workloads as wl
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    text = open(os.path.join(ROOT, "include", "sbwt_gpu.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(sbwt_\w+)\s*\(", text)))
+
+
+def test_every_declared_symbol_is_exported():
+    names = declared_functions()
+    assert len(names) >= 20
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (sbwt_\w+)", out))
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+    for n in names:
+        assert n in _lib.SIGNATURES, f"{n} has no ctypes signature"
+
+
+def test_params_default_is_the_reference_default():
+    p = sg.default_params()
+    assert (p.k, p.k_presearch, p.bits_in_superblock, p.rank_structure, p.with_shuffles) == (30, 12, 1024, 1, 0)
+
+
+def test_no_cpu_fallback_without_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(sg.SbwtError, match="no CUDA device"):
+        sg.Index.from_bits([np.zeros(1, np.uint64)] * 4, 1)
+
+
+def test_parameter_errors():
+    with pytest.raises(sg.SbwtError, match="k must be at least 3"):
+        sg.Index.from_bits([np.zeros(1, np.uint64)] * 4, 1, k=2)
+    with pytest.raises(sg.SbwtError, match="exceeds k"):
+        sg.Index.from_bits([np.zeros(1, np.uint64)] * 4, 1, k=5, k_presearch=6)
+
+
+def test_read_queries_matches_oracle(tmp_path):
+    rng = wl.rng_for(3)
+    letters, rows = wl.mixed_reads(rng, wl.random_bases(rng, 2000), 5, 5, 77, 0.01)
+    fa = tmp_path / "q.fa"
+    wl.write_fasta(str(fa), letters, rows)
+    raw = fa.read_bytes() + b">empty\n\nACG\nAC\r\nNNNNNNNNNNNNNNNNNNNNNNNNNNNNNNNNNNN\n"
+    fa.write_bytes(raw)
+    for k in (3, 31):
+        l1, r1, nk1 = sg.read_queries(str(fa), k)
+        l2, r2, nk2 = orc.read_queries(raw, k)
+        assert np.array_equal(l1, l2) and np.array_equal(r1, r2) and nk1 == nk2
+        assert sg.count_kmers(r1, k) == nk1
+
+
+def test_read_queries_keeps_last_letter_without_newline(tmp_path):
+    fa = tmp_path / "q.fa"
+    fa.write_bytes(b">x\nACGTAC")
+    letters, rows, nk = sg.read_queries(str(fa), 5)
+    assert letters.tobytes() == b"ACGTAC" and nk == 2   # the reference drops the final C here
+
+
+def test_format_answers_matches_oracle():
+    rows = np.array([0, 40, 45, 100], dtype=np.uint64)
+    k = 31
+    n = sg.count_kmers(rows, k)
+    ans = np.array([orc.NOT_FOUND if i % 3 == 0 else i * 1234567 for i in range(n)], dtype=np.uint64)
+    assert sg.format_answers(rows, k, ans) == orc.format_answers(rows, k, ans)
+    assert sg.format_answers(rows, k, ans).split(b"\n")[1] == b""  # a read shorter than k: empty line
+
+
+def test_cli_help_and_bad_flags():
+    cli = _lib.CLI_PATH
+    r = subprocess.run([cli], capture_output=True, text=True)
+    assert r.returncode == 0 and "usage" in r.stderr
+    r = subprocess.run([cli, "--rank-structure=flat-poppy", "--file-a=x"], capture_output=True, text=True)
+    assert r.returncode != 0
+    r = subprocess.run([cli, "--bits-in-superblock=4096", "--rank-structure=cum-poppy", "--file-a=a", "--file-c=c",
+                        "--file-g=g", "--file-t=t", "--file-queries=q"], capture_output=True, text=True)
+    assert r.returncode != 0 and "4096" in r.stderr

@@ -1,0 +1,277 @@
+"""CUDA path vs the oracle, bit for bit, through the C ABI (needs a B200)."""
+import gzip
+import hashlib
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as orc
+import sbwt_gpu_b200 as sg
+from sbwt_gpu_b200 import workloads as wl
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+CASES = sorted(os.listdir(os.path.join(GOLDEN, "cases")))
+
+
+def _t(a, dev):
+    import torch
+    a = np.ascontiguousarray(a)
+    if a.dtype == np.uint64:
+        a = a.view(np.int64)
+    return torch.from_numpy(a).to(dev)
+
+
+def _u64(t):
+    return t.cpu().numpy().view(np.uint64)
+
+
+@pytest.fixture(scope="module")
+def small(cuda):
+    rng = wl.rng_for(4242)
+    k = 31
+    genome = wl.random_bases(rng, 120_000)
+    built = sg.build_sbwt([genome.tobytes()], k)
+    letters, rows = wl.mixed_reads(rng, genome, 300, 300, 150, 0.01)
+    return {"k": k, "genome": genome, "built": built, "letters": letters, "rows": rows}
+
+
+def run_reads(ix, letters, rows, dev, n_kmers=None, member=False):
+    import torch
+    nk = sg.count_kmers(rows, ix.info()["k"]) if n_kmers is None else n_kmers
+    d_ans = torch.full((max(nk, 1),), -7, dtype=torch.int64, device=dev)
+    d_mem = torch.zeros(((nk + 31) // 32 + 1,), dtype=torch.int32, device=dev) if member else None
+    ix.search_reads(_t(letters, dev), _t(rows, dev), d_ans, nk, d_member_bits=d_mem)
+    torch.cuda.synchronize()
+    out = _u64(d_ans)[:nk]
+    return (out, d_mem.cpu().numpy().view(np.uint32)) if member else out
+
+
+@pytest.mark.parametrize("sb,kind", orc.SB_KINDS)
+def test_gpu_rank_build_matches_reference_layout(small, sb, kind):
+    b = small["built"]
+    ox = orc.OracleIndex(b.bits, b.n_bits, sb, kind)
+    with sg.Index.from_bits(b.bits, b.n_bits, k=31, k_presearch=0) as ix:
+        for c in range(4):
+            L0, L12 = ix.rank_structures(sb, kind, c)
+            assert np.array_equal(L0, ox.L0[c]), (sb, kind, c)
+            assert np.array_equal(L12, ox.L12[c]), (sb, kind, c)
+
+
+def test_c_array(small):
+    b = small["built"]
+    ox = orc.OracleIndex(b.bits, b.n_bits)
+    with sg.Index.from_bits(b.bits, b.n_bits, k=31) as ix:
+        assert ix.info()["C"] == [int(x) for x in ox.C]
+
+
+@pytest.mark.parametrize("p", [1, 2, 5, 9, 12])
+def test_presearch_table_matches_oracle(small, p):
+    b = small["built"]
+    ox = orc.OracleIndex(b.bits, b.n_bits)
+    with sg.Index.from_bits(b.bits, b.n_bits, k=31, k_presearch=p) as ix:
+        lefts, rights = ix.presearch_table()
+    wl_, wr = ox.presearch(p)
+    assert np.array_equal(lefts, wl_)
+    assert np.array_equal(rights, wr)
+
+
+def test_search_packed_reference_contract(small, cuda):
+    b, k = small["built"], small["k"]
+    ox = orc.OracleIndex(b.bits, b.n_bits)
+    words = orc.pack(small["letters"])
+    pos = orc.positions(small["rows"], k)
+    want = ox.search_positions(words, pos, k, 10)
+    with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=10) as ix:
+        d_words = _t(words, cuda)
+        d_pos = _t(pos, cuda)
+        ix.search_packed(d_words, d_pos)
+        import torch
+        torch.cuda.synchronize()
+        assert np.array_equal(_u64(d_pos), want)
+
+
+def test_pack_kernel_matches_oracle(cuda):
+    import torch
+    rng = np.random.default_rng(3)
+    for n in [0, 1, 31, 32, 33, 1000, 4097]:
+        letters = rng.choice(np.frombuffer(b"ACGTacgtNnRX\r>", dtype=np.uint8), size=n)
+        want = orc.pack(letters)
+        from ctypes import c_void_p
+        for off in (0, 3):  # aligned (16-byte loads) and unaligned (byte loads)
+            buf = torch.zeros(n + 64, dtype=torch.uint8, device=cuda)
+            if n:
+                buf[off:off + n] = _t(letters, cuda)
+            d_words = torch.full((want.size,), -1, dtype=torch.int64, device=cuda)
+            rc = sg._lib.lib.sbwt_pack(c_void_p(buf.data_ptr() + off), n, c_void_p(d_words.data_ptr()), None)
+            assert rc == 0
+            torch.cuda.synchronize()
+            assert np.array_equal(_u64(d_words), want), (n, off)
+
+
+SHAPES = [(kpt, tpk) for kpt in (1, 2, 3, 4, 6, 8) for tpk in (1, 2, 4)]
+
+
+@pytest.mark.parametrize("kpt,tpk", SHAPES)
+def test_search_reads_line_layout_all_shapes(small, cuda, kpt, tpk):
+    b, k = small["built"], small["k"]
+    ox = orc.OracleIndex(b.bits, b.n_bits)
+    want = ox.search_reads(small["letters"], small["rows"], k, 10)
+    with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=10) as ix:
+        ix.configure(sg.SBWT_LAYOUT_LINES, kmers_per_thread=kpt, threads_per_kmer=tpk, threads_per_block=128)
+        got = run_reads(ix, small["letters"], small["rows"], cuda)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("sb,kind", orc.SB_KINDS)
+@pytest.mark.parametrize("shuffles", [0, 1])
+def test_search_reads_poppy_layout(small, cuda, sb, kind, shuffles):
+    b, k = small["built"], small["k"]
+    ox = orc.OracleIndex(b.bits, b.n_bits)
+    want = ox.search_reads(small["letters"], small["rows"], k, 8)
+    with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=8) as ix:
+        ix.configure(sg.SBWT_LAYOUT_POPPY, bits_in_superblock=sb, rank_structure=kind, with_shuffles=shuffles,
+                     kmers_per_thread=2)
+        got = run_reads(ix, small["letters"], small["rows"], cuda)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("p", [0, 1, 4, 7, 10, 13, 15])
+def test_answers_do_not_depend_on_p(small, cuda, p):
+    b, k = small["built"], small["k"]
+    ox = orc.OracleIndex(b.bits, b.n_bits)
+    want = ox.search_reads(small["letters"], small["rows"], k, 0)
+    with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=p) as ix:
+        got = run_reads(ix, small["letters"], small["rows"], cuda)
+    assert np.array_equal(got, want)
+
+
+def test_member_bits(small, cuda):
+    b, k = small["built"], small["k"]
+    with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=10) as ix:
+        ans, bits = run_reads(ix, small["letters"], small["rows"], cuda, member=True)
+    nk = ans.size
+    want = np.zeros((nk + 31) // 32 * 32, dtype=bool)
+    want[:nk] = ans != orc.NOT_FOUND
+    w = want.reshape(-1, 32).astype(np.uint64)
+    words = (w << np.arange(32, dtype=np.uint64)).sum(axis=1).astype(np.uint32)  # bit j%32 of word j/32
+    assert np.array_equal(bits[: words.size], words)
+
+
+@pytest.mark.parametrize("k,p", [(3, 0), (3, 3), (4, 2), (9, 5), (17, 8), (25, 9), (31, 31), (32, 12), (32, 0)])
+def test_k_and_p_range(cuda, k, p):
+    rng = wl.rng_for(1000 + k)
+    genome = wl.random_bases(rng, 8000)
+    built = sg.build_sbwt([genome.tobytes()], k)
+    letters, rows = wl.mixed_reads(rng, genome, 40, 40, 70, 0.02)
+    ox = orc.OracleIndex(built.bits, built.n_bits)
+    want = ox.search_reads(letters, rows, k, min(p, 15))
+    keys, dk, _ = orc.independent_sbwt([genome.tobytes()], k)
+    assert np.array_equal(want, orc.independent_answers(keys, dk, orc.query_colex_keys(
+        orc.extract_kmers(letters, rows, k), k)))
+    with sg.Index.from_bits(built.bits, built.n_bits, k=k, k_presearch=min(p, 15)) as ix:
+        got = run_reads(ix, letters, rows, cuda)
+    assert np.array_equal(got, want)
+
+
+def test_ragged_rows_and_odd_bytes(small, cuda):
+    """Reads shorter than k, empty reads, N and lowercase letters, one-letter reads."""
+    b, k = small["built"], small["k"]
+    rng = np.random.default_rng(11)
+    g = small["genome"]
+    parts = [g[100:400], np.frombuffer(b"ACG", np.uint8), np.zeros(0, np.uint8), g[5000:5031],
+             np.frombuffer(b"NNNNNNNNNNNNNNNNNNNNNNNNNNNNNNNNNNNNNN", np.uint8),
+             np.frombuffer(g[7000:7100].tobytes().lower(), np.uint8), g[9000:9030], np.frombuffer(b"A", np.uint8),
+             rng.choice(np.frombuffer(b"ACGTN", np.uint8), size=500)]
+    letters = np.concatenate(parts)
+    rows = np.zeros(len(parts) + 1, dtype=np.uint64)
+    rows[1:] = np.cumsum([p.size for p in parts])
+    ox = orc.OracleIndex(b.bits, b.n_bits)
+    want = ox.search_reads(letters, rows, k, 10)
+    with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=10) as ix:
+        got = run_reads(ix, letters, rows, cuda)
+        host = ix.search_reads_host(letters, rows)
+    assert np.array_equal(got, want)
+    assert np.array_equal(host, want)
+    assert (want[: 300 - k + 1] != orc.NOT_FOUND).all()  # an exact genome substring is present
+
+
+def test_n_kmers_smaller_than_rows_hold(small, cuda):
+    b, k = small["built"], small["k"]
+    ox = orc.OracleIndex(b.bits, b.n_bits)
+    want = ox.search_reads(small["letters"], small["rows"], k, 10)
+    with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=10) as ix:
+        got = run_reads(ix, small["letters"], small["rows"], cuda, n_kmers=1000)
+    assert np.array_equal(got, want[:1000])
+
+
+def test_search_reads_host_pinned_and_pageable(small, cuda):
+    import torch
+    b, k = small["built"], small["k"]
+    ox = orc.OracleIndex(b.bits, b.n_bits)
+    want = ox.search_reads(small["letters"], small["rows"], k, 10)
+    with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=10) as ix:
+        got = ix.search_reads_host(small["letters"], small["rows"])
+        assert np.array_equal(got, want)
+        pl = torch.from_numpy(small["letters"]).pin_memory()
+        pr = torch.from_numpy(small["rows"].view(np.int64)).pin_memory()
+        pa = torch.empty(want.size, dtype=torch.int64).pin_memory()
+        ix.search_reads_host(pl, pr, pa)
+        assert np.array_equal(pa.numpy().view(np.uint64), want)
+
+
+def test_config1_full_workload(cuda, tmp_path):
+    import make_golden
+    n, letters, rows = make_golden.write_config1(str(tmp_path))
+    paths = [str(tmp_path / f"ix.{c}") for c in "ACGT"]
+    ox = orc.OracleIndex.from_files(paths)
+    want = ox.search_reads(letters, rows, 31, 10)
+    with sg.Index.load(*paths, k=31, k_presearch=10) as ix:
+        got = run_reads(ix, letters, rows, cuda)
+        host = ix.search_reads_host(letters, rows)
+    assert np.array_equal(got, want)
+    assert np.array_equal(host, want)
+    meta_p = os.path.join(GOLDEN, "config1.json")
+    if os.path.exists(meta_p):
+        text = sg.format_answers(rows, 31, got)
+        assert hashlib.sha256(text).hexdigest() == json.load(open(meta_p))["reference_sha256"]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_cli_matches_reference_program(case, cuda):
+    d = os.path.join(GOLDEN, "cases", case)
+    meta = json.load(open(os.path.join(d, "case.json")))
+    import make_golden
+    flags = make_golden.case_flags(case, os.path.join(GOLDEN, "cases"))
+    ref_path = os.path.join(d, "reference.out.gz")
+    if os.path.exists(ref_path):
+        want = gzip.open(ref_path).read()
+    else:
+        kind = orc.POPPY if meta["rank_structure"] == "poppy" else orc.CUM_POPPY
+        ox = orc.OracleIndex.from_files([os.path.join(d, f"ix.{c}") for c in "ACGT"], meta["bits_in_superblock"],
+                                        kind)
+        letters, rows, _ = orc.read_queries(open(os.path.join(d, "queries.fa"), "rb").read(), meta["k"])
+        want = orc.format_answers(rows, meta["k"], ox.search_reads(letters, rows, meta["k"], meta["p"]))
+    for layout in ("lines", "poppy"):
+        r = subprocess.run([sg.CLI_PATH] + flags + [f"--layout={layout}"], capture_output=True, timeout=300)
+        assert r.returncode == 0, r.stderr.decode()
+        assert r.stdout == want, (case, layout)
+
+
+def test_index_load_errors(tmp_path, cuda):
+    b = sg.build_sbwt(["ACGTACGTTTGACCA" * 3], 5)
+    paths = sg.write_index_files(str(tmp_path / "ix"), b)
+    other = sg.build_sbwt(["ACGTACGTTTGACCAGG" * 3], 5)
+    p2 = sg.write_index_files(str(tmp_path / "other"), other)
+    with pytest.raises(sg.SbwtError, match="different lengths"):
+        sg.Index.load(paths[0], paths[1], paths[2], p2[3], k=5, k_presearch=0)
+    with pytest.raises(sg.SbwtError):
+        sg.Index.load(paths[0], paths[1], paths[2], str(tmp_path / "missing"), k=5)
+    bad = tmp_path / "bad"
+    bad.write_bytes((10_000).to_bytes(8, "little") + b"\0" * 10)
+    with pytest.raises(sg.SbwtError):
+        sg.Index.load(str(bad), str(bad), str(bad), str(bad), k=5)
