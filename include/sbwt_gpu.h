@@ -115,6 +115,21 @@ int sbwt_configure(sbwt_index *index, int32_t layout, uint32_t bits_in_superbloc
                    int32_t with_shuffles, uint32_t kmers_per_thread, uint32_t threads_per_kmer,
                    uint32_t threads_per_block);
 
+/* Sets the L2 fetch granularity (32, 64 or 128 bytes; cudaLimitMaxL2FetchGranularity)
+ * of the index's device for this process, as the reference does before its
+ * presearch and search kernels (include/presearch.hpp:34-37,
+ * include/epicseq/search_caller.hpp:91-96, flags --device-set-limit-presearch
+ * and --device-set-limit-search). */
+int sbwt_set_l2_fetch_granularity(sbwt_index *index, uint32_t bytes);
+
+/* Turns CUDA-graph replay of sbwt_search_reads on or off (default off).
+ * When on, a call on a non-default stream captures its whole kernel chain
+ * (pack -> per-row table -> search -> bitmap) into a CUDA graph, and a later
+ * call with the same buffers, sizes and launch shape replays that graph with
+ * one launch.  No reference counterpart (the reference launches each kernel
+ * separately, include/epicseq/kmer_search.hpp:97-160). */
+int sbwt_use_graphs(sbwt_index *index, int on);
+
 /* ----------------------------------------------------------------- search */
 
 /* The reference kernel contract: d_kmer_string holds the packed letters
@@ -178,6 +193,22 @@ int sbwt_profile_read(sbwt_index *index, sbwt_profile *out);
 /* Number of k-mers in a batch of rows (sum of max(0, len-k+1)). */
 uint64_t sbwt_count_kmers(const uint64_t *row_starts, uint64_t n_rows, uint32_t k);
 
+/* Autotuner (no reference counterpart; the reference takes its kernel
+ * variant from flags, include/parameters.hpp:79-297).  Times
+ * sbwt_search_reads on the given device sample for every candidate launch
+ * shape (line layout x k-mers per thread {1,2,3,4,6,8} x threads per k-mer
+ * {1,2,4} x threads per block {128,256}; with SBWT_TUNE_POPPY also the poppy
+ * layouts SB 512/1024/2048 with and without shuffles; with SBWT_TUNE_P also
+ * presearch depths {8,10,12,14} <= k), checks that every candidate's answers
+ * have the same checksum, and leaves the fastest configured on the index.
+ * d_answers: device scratch of n_kmers u64.  report (optional): JSON of all
+ * timings (fails if report_cap is too small). */
+#define SBWT_TUNE_P 2u
+#define SBWT_TUNE_POPPY 4u
+int sbwt_autotune(sbwt_index *index, const uint8_t *d_letters, uint64_t n_letters, const uint64_t *d_row_starts,
+                  uint64_t n_rows, uint64_t n_kmers, uint64_t *d_answers, uint32_t flags, char *report,
+                  uint64_t report_cap);
+
 /* ------------------------------------------------------------ query files */
 
 /* Reads a FASTA query file the way KmerSearch::read_file does
@@ -194,6 +225,13 @@ typedef struct {
 } sbwt_queries;
 
 int sbwt_queries_read(const char *path, uint32_t k, sbwt_queries *out);
+
+/* Reads n_files query files (in parallel) into one batch: rows of file f are
+ * rows [file_rows[f], file_rows[f+1]) of *out (file_rows: n_files + 1
+ * entries).  One batch means one persistent search launch over all files.
+ * No reference counterpart (the reference takes one query file,
+ * include/parameters.hpp:29). */
+int sbwt_queries_read_many(const char *const *paths, int n_files, uint32_t k, sbwt_queries *out, uint64_t *file_rows);
 void sbwt_queries_free(sbwt_queries *q);
 
 /* Formats answers as the reference prints them (results_persister.hpp:82-95):

@@ -23,7 +23,7 @@ from ._lib import (CLI_PATH, LIB_PATH, SBWT_CUM_POPPY, SBWT_LAYOUT_LINES, SBWT_L
 
 __all__ = [
     "Index", "Params", "SbwtError", "build_sbwt", "write_index_files", "read_queries", "format_answers",
-    "count_kmers", "default_params", "SBWT_POPPY", "SBWT_CUM_POPPY", "SBWT_LAYOUT_LINES", "SBWT_LAYOUT_POPPY",
+    "count_kmers", "read_queries_many", "default_params", "SBWT_POPPY", "SBWT_CUM_POPPY", "SBWT_LAYOUT_LINES", "SBWT_LAYOUT_POPPY",
     "LIB_PATH", "CLI_PATH", "NOT_FOUND",
 ]
 
@@ -139,6 +139,24 @@ class Index:
         check(lib.sbwt_configure(self._h, layout, bits_in_superblock, rank_structure, int(with_shuffles),
                                  kmers_per_thread, threads_per_kmer, threads_per_block))
 
+    def autotune(self, d_letters, d_row_starts, d_answers, n_kmers, tune_p=False, tune_poppy=False):
+        """Times candidate launch shapes on a device sample, keeps the fastest; returns the JSON report."""
+        n_rows = int(d_row_starts.numel()) - 1
+        flags = (2 if tune_p else 0) | (4 if tune_poppy else 0)
+        buf = ctypes.create_string_buffer(1 << 16)
+        check(lib.sbwt_autotune(self._h, _ptr(d_letters), int(d_letters.numel()), _ptr(d_row_starts), n_rows,
+                                int(n_kmers), _ptr(d_answers), flags, buf, len(buf)))
+        import json
+        return json.loads(buf.value.decode())
+
+    def set_l2_fetch_granularity(self, nbytes):
+        """cudaLimitMaxL2FetchGranularity for this process (the reference's --device-set-limit-search)."""
+        check(lib.sbwt_set_l2_fetch_granularity(self._h, int(nbytes)))
+
+    def use_graphs(self, on=True):
+        """CUDA-graph replay of repeated sbwt_search_reads calls (same buffers and sizes)."""
+        check(lib.sbwt_use_graphs(self._h, int(on)))
+
     def profile(self, on=True):
         """Enables CUDA-event timing of each sbwt_search_reads phase."""
         check(lib.sbwt_profile_enable(self._h, int(on)))
@@ -238,6 +256,22 @@ def read_queries(path, k):
     finally:
         lib.sbwt_queries_free(byref(q))
     return letters, rows, nk
+
+
+def read_queries_many(paths, k):
+    """Several query files as one batch: (letters, row_starts, n_kmers, file_rows)."""
+    arr = (ctypes.c_char_p * len(paths))(*[os.fsencode(p) for p in paths])
+    file_rows = np.zeros(len(paths) + 1, dtype=np.uint64)
+    q = Queries()
+    check(lib.sbwt_queries_read_many(arr, len(paths), int(k), byref(q), _ptr(file_rows)))
+    try:
+        letters = np.ctypeslib.as_array(q.letters, shape=(q.n_letters + 32,))[: q.n_letters].copy() \
+            if q.n_letters else np.zeros(0, dtype=np.uint8)
+        rows = np.ctypeslib.as_array(q.row_starts, shape=(q.n_rows + 1,)).copy()
+        nk = int(q.n_kmers)
+    finally:
+        lib.sbwt_queries_free(byref(q))
+    return letters, rows, nk, file_rows
 
 
 def count_kmers(row_starts, k):

@@ -91,8 +91,13 @@ SIGNATURES = {
     "sbwt_search_reads_host": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_void_p, c_uint64]),
     "sbwt_count_kmers": (c_uint64, [c_void_p, c_uint64, c_uint32]),
     "sbwt_profile_enable": (c_int, [c_void_p, c_int]),
+    "sbwt_use_graphs": (c_int, [c_void_p, c_int]),
+    "sbwt_set_l2_fetch_granularity": (c_int, [c_void_p, c_uint32]),
     "sbwt_profile_read": (c_int, [c_void_p, POINTER(Profile)]),
     "sbwt_queries_read": (c_int, [c_char_p, c_uint32, POINTER(Queries)]),
+    "sbwt_queries_read_many": (c_int, [POINTER(c_char_p), c_int, c_uint32, POINTER(Queries), c_void_p]),
+    "sbwt_autotune": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_uint64, c_void_p, c_uint32, c_void_p,
+                              c_uint64]),
     "sbwt_queries_free": (None, [POINTER(Queries)]),
     "sbwt_format_answers": (c_int64, [c_void_p, c_uint64, c_uint32, c_void_p, c_void_p, c_uint64]),
     "sbwt_build": (c_int, [c_void_p, c_void_p, c_uint64, c_uint32, POINTER(Built)]),

@@ -21,6 +21,7 @@ void Workspace::release() {
     if (h_rows) cudaFreeHost(h_rows);
     if (h_letters) cudaFreeHost(h_letters);
     if (h_answers) cudaFreeHost(h_answers);
+    if (graph) cudaGraphExecDestroy(graph);
     *this = Workspace();
 }
 
@@ -373,6 +374,9 @@ SearchArgs base_args(const sbwt_index *ix) {
 }  // namespace
 
 // Device-resident batch of rows on stream s using workspace w.
+int enqueue_rows(sbwt_index *ix, Workspace &w, SearchArgs &a, const uint8_t *d_letters, u64 n_letters, const u64 *d_rows,
+                 u64 n_rows, u64 *d_answers, uint32_t *d_member, u64 n_kmers, cudaStream_t s, bool prof);
+
 int search_rows_device(sbwt_index *ix, Workspace &w, const uint8_t *d_letters, u64 n_letters, const u64 *d_rows,
                        u64 n_rows, u64 *d_answers, uint32_t *d_member, u64 n_kmers, cudaStream_t s) {
     if (n_rows == 0 || n_kmers == 0) return 0;
@@ -384,6 +388,50 @@ int search_rows_device(sbwt_index *ix, Workspace &w, const uint8_t *d_letters, u
     SBWT_TRY(grow(w.chunk_row, w.chunk_cap, (n_kmers + a.chunk - 1) / a.chunk));
     SBWT_TRY(grow(w.counter, w.counter_cap, 1));
     const bool prof = ix->prof_on;
+    // CUDA graph: the whole chain is captured once and replayed while its
+    // parameters stay the same (not on the legacy default stream, not while
+    // profiling per phase)
+    bool capturing = false;
+    if (ix->use_graph && !prof && s != nullptr) {
+        const KernelShape &sh = ix->shape;
+        const uint64_t key[12] = {(uint64_t)d_letters, n_letters, (uint64_t)d_rows, n_rows, (uint64_t)d_answers,
+                                  (uint64_t)d_member, n_kmers, (uint64_t)s, ix->gen,
+                                  ((uint64_t)sh.layout << 48) | ((uint64_t)sh.kpt << 32) | ((uint64_t)sh.tpk << 16) | sh.tpb,
+                                  (uint64_t)w.words ^ (uint64_t)w.kstart, (uint64_t)w.chunk_row ^ (uint64_t)w.counter};
+        if (w.graph && std::memcmp(key, w.graph_key, sizeof key) == 0) {
+            SBWT_CHECK_CUDA(cudaGraphLaunch(w.graph, s));
+            return 0;
+        }
+        if (w.graph) cudaGraphExecDestroy(w.graph);
+        w.graph = nullptr;
+        std::memcpy(w.graph_key, key, sizeof key);
+        SBWT_CHECK_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        capturing = true;
+    }
+    const int rc = enqueue_rows(ix, w, a, d_letters, n_letters, d_rows, n_rows, d_answers, d_member, n_kmers, s, prof);
+    if (capturing) {
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(s, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (e != cudaSuccess) return set_error("graph capture failed: %s", cudaGetErrorString(e));
+        const cudaError_t ei = cudaGraphInstantiate(&w.graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            w.graph = nullptr;
+            return set_error("graph instantiation failed: %s", cudaGetErrorString(ei));
+        }
+        SBWT_CHECK_CUDA(cudaGraphLaunch(w.graph, s));
+    }
+    return rc;
+}
+
+// The kernels of one batch, in stream order.
+int enqueue_rows(sbwt_index *ix, Workspace &w, SearchArgs &a, const uint8_t *d_letters, u64 n_letters, const u64 *d_rows,
+                 u64 n_rows, u64 *d_answers, uint32_t *d_member, u64 n_kmers, cudaStream_t s, bool prof) {
+    const u64 n_words = (n_letters + 32 + 31) / 32;
     if (prof) SBWT_CHECK_CUDA(cudaEventRecord(ix->prof_ev[0], s));
     SBWT_TRY(launch_pack(d_letters, n_letters, w.words, s));
     if (prof) SBWT_CHECK_CUDA(cudaEventRecord(ix->prof_ev[1], s));
@@ -453,6 +501,22 @@ extern "C" int sbwt_search_reads(sbwt_index *ix, const uint8_t *d_letters, uint6
     SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
     return search_rows_device(ix, ix->ws[0], d_letters, n_letters, d_row_starts, n_rows, d_answers, d_member_bits,
                               n_kmers, (cudaStream_t)stream);
+}
+
+extern "C" int sbwt_set_l2_fetch_granularity(sbwt_index *ix, uint32_t bytes) {
+    clear_error();
+    if (!ix) return set_error("index is NULL");
+    if (bytes != 32 && bytes != 64 && bytes != 128) return set_error("the L2 fetch granularity must be 32, 64 or 128");
+    SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
+    SBWT_CHECK_CUDA(cudaDeviceSetLimit(cudaLimitMaxL2FetchGranularity, bytes));
+    return 0;
+}
+
+extern "C" int sbwt_use_graphs(sbwt_index *ix, int on) {
+    clear_error();
+    if (!ix) return set_error("index is NULL");
+    ix->use_graph = on != 0;
+    return 0;
 }
 
 extern "C" int sbwt_profile_enable(sbwt_index *ix, int on) {

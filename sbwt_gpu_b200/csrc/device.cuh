@@ -92,6 +92,39 @@ __device__ __forceinline__ u32 line_rank_from(const ulonglong4 &w, u32 q) {
     return (u32)(w.x >> 32) + line_prefix(w, q);
 }
 
+// Per-line running popcounts, shared by every rank taken in that line:
+// count = ones before the line, p1..p3 = ones in line words 0 (data half),
+// 0..1 and 0..2.
+struct LineSums {
+    u32 count, p1, p2, p3;
+    u64 w0, w1, w2, w3;
+};
+
+__device__ __forceinline__ LineSums line_sums(const ulonglong4 &w) {
+    LineSums s;
+    s.count = (u32)(w.x >> 32);
+    s.w0 = w.x & 0xffffffffull;
+    s.w1 = w.y;
+    s.w2 = w.z;
+    s.w3 = w.w;
+    s.p1 = __popcll(s.w0);
+    s.p2 = s.p1 + __popcll(s.w1);
+    s.p3 = s.p2 + __popcll(s.w2);
+    return s;
+}
+
+// rank at data position q (< 224) of the line: the full words before the one
+// holding q come from the running sums, that word is masked by one clamped
+// shift.  *bit = the bit at q itself.
+__device__ __forceinline__ u32 sums_rank(const LineSums &s, u32 q, u32 &bit) {
+    const u32 t = q + 32u;  // line bit of q
+    const u32 wi = t >> 6, b = t & 63u;
+    const u32 full = wi == 0 ? 0u : wi == 1 ? s.p1 : wi == 2 ? s.p2 : s.p3;
+    const u64 w = wi == 0 ? s.w0 : wi == 1 ? s.w1 : wi == 2 ? s.w2 : s.w3;
+    bit = (u32)(w >> (63u - b)) & 1u;
+    return s.count + full + __popcll(shr_clamp(w, 64u - b));
+}
+
 __device__ __forceinline__ void line_split(u32 x, u32 &line, u32 &q) {
     line = x / kLineBits;
     q = x - line * kLineBits;

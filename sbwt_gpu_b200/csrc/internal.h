@@ -64,6 +64,10 @@ struct Workspace {
     uint64_t *h_rows = nullptr; size_t h_rows_cap = 0;  // pinned host staging
     uint8_t *h_letters = nullptr; size_t h_letters_cap = 0;
     uint64_t *h_answers = nullptr; size_t h_answers_cap = 0;
+    // CUDA graph of the last pack -> table -> search -> bitmap chain, replayed
+    // while every launch parameter (the key) stays the same
+    cudaGraphExec_t graph = nullptr;
+    uint64_t graph_key[12] = {0};
     void release();
 };
 
@@ -101,6 +105,9 @@ struct sbwt_index {
     // ws[0] and ws[1] the two streams of the host pipeline
     sbwt::Workspace ws[2];
     cudaStream_t pipe_stream[2] = {nullptr, nullptr};
+    // bumped whenever a device structure a search reads is rebuilt (graph keys)
+    uint64_t gen = 1;
+    bool use_graph = false;
     // per-call profiling (sbwt_profile_enable)
     bool prof_on = false;
     cudaEvent_t prof_ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};

@@ -88,6 +88,7 @@ int run_poppy_levels(sbwt_index *ix, u32 p, void *table, cudaStream_t s) {
 }  // namespace
 
 int run_presearch(sbwt_index *ix, uint32_t p, cudaStream_t s) {
+    ix->gen++;
     if (ix->d_pre) cudaFree(ix->d_pre);
     ix->d_pre = nullptr;
     ix->p = 0;

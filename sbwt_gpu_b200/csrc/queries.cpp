@@ -6,6 +6,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <string>
 #include <vector>
 
 #include "sbwt_gpu.h"
@@ -133,4 +134,57 @@ extern "C" int64_t sbwt_format_answers(const uint64_t *row_starts, uint64_t n_ro
         o += 1;
     }
     return (int64_t)o;
+}
+
+extern "C" int sbwt_queries_read_many(const char *const *paths, int n_files, uint32_t k, sbwt_queries *out,
+                                      uint64_t *file_rows) {
+    sbwt::clear_error();
+    if (!out || !paths || n_files <= 0) return sbwt::set_error("sbwt_queries_read_many: bad arguments");
+    std::memset(out, 0, sizeof(*out));
+    std::vector<sbwt_queries> parts((size_t)n_files);
+    std::vector<int> rc((size_t)n_files, 0);
+    std::vector<std::string> err((size_t)n_files);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int f = 0; f < n_files; f++) {
+        rc[f] = sbwt_queries_read(paths[f], k, &parts[f]);
+        if (rc[f]) err[f] = sbwt::last_error();
+    }
+    int bad = -1;
+    for (int f = 0; f < n_files; f++)
+        if (rc[f] && bad < 0) bad = f;
+    uint64_t nl = 0, nr = 0, nk = 0;
+    for (int f = 0; f < n_files && bad < 0; f++) {
+        nl += parts[f].n_letters;
+        nr += parts[f].n_rows;
+        nk += parts[f].n_kmers;
+    }
+    uint8_t *letters = bad < 0 ? (uint8_t *)std::malloc(nl + 64) : nullptr;
+    uint64_t *rows = bad < 0 ? (uint64_t *)std::malloc((nr + 1) * sizeof(uint64_t)) : nullptr;
+    if (bad < 0 && (!letters || !rows)) bad = n_files;
+    if (bad >= 0) {
+        for (auto &q : parts) sbwt_queries_free(&q);
+        std::free(letters);
+        std::free(rows);
+        if (bad == n_files) return sbwt::set_error("out of host memory");
+        return sbwt::set_error("%s", err[(size_t)bad].c_str());
+    }
+    uint64_t lo = 0, ro = 0;
+    for (int f = 0; f < n_files; f++) {
+        const sbwt_queries &q = parts[f];
+        if (file_rows) file_rows[f] = ro;
+        if (q.n_letters) std::memcpy(letters + lo, q.letters, q.n_letters);
+        for (uint64_t r = 0; r < q.n_rows; r++) rows[ro + r] = q.row_starts[r] + lo;
+        lo += q.n_letters;
+        ro += q.n_rows;
+        sbwt_queries_free(&parts[f]);
+    }
+    if (file_rows) file_rows[n_files] = ro;
+    rows[nr] = nl;
+    std::memset(letters + nl, 0, 32);
+    out->letters = letters;
+    out->n_letters = nl;
+    out->row_starts = rows;
+    out->n_rows = nr;
+    out->n_kmers = nk;
+    return 0;
 }

@@ -23,19 +23,21 @@ struct LinesRankerT {
     const ulonglong4 *lines;
     u32 lpc;
 
+    // TPK == 1: whole lines in registers.  A single-node interval (l == r, the
+    // common case once a k-mer is matched) needs one line: rank(r+1) =
+    // rank(l) + bit(l), whichever line l+1 falls in.
     struct Fetch {
-        u64 a[W], b[W];
+        ulonglong4 a, b;
+        u64 pa[W], pb[W];  // TPK > 1: this lane's words
         u32 qa, qb;
-        bool two;
+        bool two, single;
     };
 
-    __device__ __forceinline__ static void load(const ulonglong4 *line, u32 sub, u64 (&w)[W]) {
-        if constexpr (TPK == 1) {
-            const ulonglong4 v = ld_line(line);
-            w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w;
-        } else if constexpr (TPK == 2) {
+    __device__ __forceinline__ static void load_part(const ulonglong4 *line, u32 sub, u64 (&w)[W]) {
+        if constexpr (TPK == 2) {
             const ulonglong2 v = ld_nc2(reinterpret_cast<const ulonglong2 *>(line) + sub);
-            w[0] = v.x; w[1] = v.y;
+            w[0] = v.x;
+            w[1] = v.y;
         } else {
             w[0] = ld_nc(reinterpret_cast<const u64 *>(line) + sub);
         }
@@ -59,22 +61,43 @@ struct LinesRankerT {
         u32 la, lb;
         line_split(l, la, f.qa);
         line_split(r + 1u, lb, f.qb);
-        load(base + la, sub, f.a);
         f.two = lb != la;
-        if (f.two) load(base + lb, sub, f.b);
+        if constexpr (TPK == 1) {
+            f.single = l == r;
+            f.a = ld_line(base + la);
+            if (!f.single && f.two) f.b = ld_line(base + lb);
+        } else {
+            f.single = false;
+            load_part(base + la, sub, f.pa);
+            if (f.two) load_part(base + lb, sub, f.pb);
+        }
         return f;
     }
 
     __device__ __forceinline__ void finish(const Fetch &f, u32 Cc, u32 &l, u32 &r, u32 sub, u32 gmask) const {
-        u32 ra = part(f.a, sub, f.qa);
-        u32 rb = f.two ? part(f.b, sub, f.qb) : part(f.a, sub, f.qb);
+        if constexpr (TPK == 1) {
+            const LineSums sa = line_sums(f.a);
+            u32 bit;
+            const u32 ra = sums_rank(sa, f.qa, bit);
+            l = Cc + ra;
+            if (f.single) {
+                r = Cc + ra + bit - 1u;
+            } else {
+                u32 bb;
+                const u32 rb = f.two ? sums_rank(line_sums(f.b), f.qb, bb) : sums_rank(sa, f.qb, bb);
+                r = Cc + rb - 1u;
+            }
+        } else {
+            u32 ra = part(f.pa, sub, f.qa);
+            u32 rb = f.two ? part(f.pb, sub, f.qb) : part(f.pa, sub, f.qb);
 #pragma unroll
-        for (int o = 1; o < TPK; o <<= 1) {
-            ra += __shfl_xor_sync(gmask, ra, o);
-            rb += __shfl_xor_sync(gmask, rb, o);
+            for (int o = 1; o < TPK; o <<= 1) {
+                ra += __shfl_xor_sync(gmask, ra, o);
+                rb += __shfl_xor_sync(gmask, rb, o);
+            }
+            l = Cc + ra;
+            r = Cc + rb - 1u;
         }
-        l = Cc + ra;
-        r = Cc + rb - 1u;
     }
 
     __device__ __forceinline__ void step(u32 c, u32 Cc, u32 &l, u32 &r) const {

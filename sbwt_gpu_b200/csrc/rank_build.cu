@@ -199,6 +199,7 @@ int build_poppy(sbwt_index *ix, uint32_t sb, int kind, cudaStream_t s) {
         return set_error("rank_structure must be poppy (1) or cum_poppy (2) (got %d)", kind);
     if (sb == 4096 && kind != SBWT_POPPY)
         return set_error("Superblock size 4096 bits is supported only in the rank structure version poppy.");
+    ix->gen++;
     const u32 log_hyper = sb == 4096 ? 31 : 32;
     const u64 l0w = 1ull + (ix->n >> log_hyper);                  // rank_data_structures.hpp:67
     const u64 l12w = 1ull + ((ix->n + sb - 1ull) / sb * sb) / sb;  // rank_data_structures.hpp:68

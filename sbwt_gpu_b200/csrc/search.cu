@@ -41,8 +41,12 @@ template <class IT> struct PairOf;
 template <> struct PairOf<u32> { using T = uint2; };
 template <> struct PairOf<u64> { using T = ulonglong2; };
 
+// Register budget per k-mer slot count: at least this many 256-thread blocks
+// stay resident per SM.
+template <int KPT> struct MinBlocks { static constexpr int value = KPT <= 1 ? 4 : KPT == 2 ? 3 : KPT <= 4 ? 2 : 1; };
+
 template <class R, int KPT, int TPK>
-__global__ void __launch_bounds__(256) search_kernel(const R rk, const SearchArgs a) {
+__global__ void __launch_bounds__(256, MinBlocks<KPT>::value) search_kernel(const R rk, const SearchArgs a) {
     using IT = typename R::IT;
     using PT = typename PairOf<IT>::T;
     const u32 lane = threadIdx.x & 31u;

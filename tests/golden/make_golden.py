@@ -21,6 +21,7 @@ sets MALLOC_PERTURB_=255, which makes glibc hand out zero-filled memory.
 """
 import gzip
 import hashlib
+import re
 import json
 import os
 import shutil
@@ -133,14 +134,21 @@ def run(out_dir):
     shutil.rmtree(c1)
 
 
+def reference_failed(err):
+    """The reference's error reports (include/gpu/cuda.hpp:67-84, search_caller.hpp:68-71)."""
+    return (b"did not succeed" in err or re.search(rb"CUDA error \d+ \(", err) is not None
+            or re.search(rb"Last CUDA error code [1-9]", err) is not None)
+
+
 def collect(out_dir):
     for name in SPECS:
         src = os.path.join(out_dir, f"{name}.out")
         err = open(os.path.join(out_dir, f"{name}.err"), "rb").read()
-        if b"did not succeed" in err or b"CUDA error" in err:
+        if reference_failed(err):
             raise SystemExit(f"{name}: the reference reported an error")
         data = open(src, "rb").read()
-        with gzip.open(os.path.join(CASES, name, "reference.out.gz"), "wb", mtime=0) as f:
+        with open(os.path.join(CASES, name, "reference.out.gz"), "wb") as raw, \
+                gzip.GzipFile(fileobj=raw, mode="wb", mtime=0) as f:
             f.write(data)
         meta_p = os.path.join(CASES, name, "case.json")
         meta = json.load(open(meta_p))
@@ -148,7 +156,7 @@ def collect(out_dir):
         json.dump(meta, open(meta_p, "w"), indent=1)
         print(name, len(data), "bytes")
     err = open(os.path.join(out_dir, "config1.err"), "rb").read()
-    if b"did not succeed" in err or b"CUDA error" in err:
+    if reference_failed(err):
         raise SystemExit("config1: the reference reported an error")
     data = open(os.path.join(out_dir, "config1.out"), "rb").read()
     json.dump({"seed": CONFIG1_SEED, "bytes": len(data), "lines": data.count(b"\n"),

@@ -1,0 +1,76 @@
+"""Times the reference's own CUDA search kernel (oracle/_ref/search: the
+reference program built for sm_100a) on the large benchmark workload, from
+the kernel time the reference itself prints ("Search in GPU: X ms",
+include/epicseq/kmer_search.hpp:167-169; CUDA events around the kernel,
+include/gpu/search_and_presearch_launchers.hpp:41,53-54).
+
+    python tests/golden/reference_gpu_timing.py [--scale S] [--out FILE]
+
+The inputs satisfy the reference's in-bounds conditions (make_golden.check_safe):
+150 bp ACGT reads, a k-mer count that is a multiple of 64 with
+--threads-per-block=64, p = 12, n not a multiple of 4096.  The answers are
+not printed (--do-not-store-results).  Test infrastructure only.
+"""
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, HERE)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--out", default=None)
+    args = ap.parse_args()
+    import bench
+    import make_golden
+    import sbwt_gpu_b200 as sg
+    from sbwt_gpu_b200 import workloads as wl
+    genome, letters, rows = bench.workload(args.scale, 0)
+    built = sg.build_sbwt([genome.tobytes()], 31)
+    make_golden.check_safe(built.n_bits, letters, rows, 31, 12)
+    d = tempfile.mkdtemp(prefix="sbwt_ref_")
+    sg.write_index_files(os.path.join(d, "ix"), built)
+    n_bits = built.n_bits
+    del built, genome
+    wl.write_fasta(os.path.join(d, "queries.fa"), letters, rows)
+    flags = make_golden.config1_flags(d)
+    flags = [f for f in flags if not f.startswith("--k-presearch")] + ["--k-presearch=12", "--do-not-store-results"]
+    env = dict(os.environ, MALLOC_PERTURB_="255")
+    r = subprocess.run([make_golden.REF_SEARCH] + flags, capture_output=True, env=env, timeout=3600)
+    err = r.stderr.decode(errors="replace")
+    if r.returncode != 0 or make_golden.reference_failed(r.stderr):
+        print(err[-3000:])
+        raise SystemExit("the reference reported an error")
+
+    def grab(pattern):
+        m = re.search(pattern, err)
+        return float(m.group(1)) if m else None
+
+    n_kmers = int((rows[1:] - rows[:-1]).astype("int64").sum() - (rows.size - 1) * 30)
+    res = {
+        "workload": f"large x{args.scale}", "n_kmers": n_kmers, "n_columns": n_bits,
+        "search_ms": grab(r"Search in GPU: ([0-9.]+) ms"),
+        "presearch_ms": grab(r"Presearch takes ([0-9.]+) ms"),
+        "pack_ms": grab(r"IN GPU: ([0-9.]+) ms"),
+        "total_per_query_ns": grab(r"Total per query: ([0-9.]+) ns"),
+        "flags": " ".join(f for f in flags if not f.startswith("--file")),
+    }
+    res["search_kmers_per_s"] = n_kmers / (res["search_ms"] / 1e3) if res["search_ms"] else None
+    line = json.dumps(res)
+    print(line)
+    if args.out:
+        with open(args.out, "w") as f:
+            f.write(line + "\n")
+
+
+if __name__ == "__main__":
+    main()

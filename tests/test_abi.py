@@ -91,3 +91,24 @@ def test_cli_help_and_bad_flags():
     r = subprocess.run([cli, "--bits-in-superblock=4096", "--rank-structure=cum-poppy", "--file-a=a", "--file-c=c",
                         "--file-g=g", "--file-t=t", "--file-queries=q"], capture_output=True, text=True)
     assert r.returncode != 0 and "4096" in r.stderr
+
+
+def test_read_queries_many_concatenates(tmp_path):
+    rng = wl.rng_for(21)
+    paths, parts = [], []
+    for f in range(4):
+        letters, rows = wl.mixed_reads(rng, wl.random_bases(rng, 3000), 3 + f, 2, 50 + 10 * f, 0.0)
+        p = str(tmp_path / f"f{f}.fa")
+        wl.write_fasta(p, letters, rows)
+        paths.append(p)
+        parts.append(sg.read_queries(p, 31))
+    letters, rows, nk, file_rows = sg.read_queries_many(paths, 31)
+    assert np.array_equal(letters, np.concatenate([p[0] for p in parts]))
+    assert nk == sum(p[2] for p in parts)
+    assert file_rows.tolist() == np.cumsum([0] + [p[1].size - 1 for p in parts]).tolist()
+    off = 0
+    for f, p in enumerate(parts):
+        r0, r1 = int(file_rows[f]), int(file_rows[f + 1])
+        assert np.array_equal(rows[r0:r1 + 1] - rows[r0], p[1])
+    with pytest.raises(sg.SbwtError):
+        sg.read_queries_many(paths + [str(tmp_path / "missing.fa")], 31)

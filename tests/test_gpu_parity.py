@@ -275,3 +275,70 @@ def test_index_load_errors(tmp_path, cuda):
     bad.write_bytes((10_000).to_bytes(8, "little") + b"\0" * 10)
     with pytest.raises(sg.SbwtError):
         sg.Index.load(str(bad), str(bad), str(bad), str(bad), k=5)
+
+
+def test_autotune_keeps_answers_and_picks_a_shape(small, cuda):
+    import torch
+    b, k = small["built"], small["k"]
+    ox = orc.OracleIndex(b.bits, b.n_bits)
+    want = ox.search_reads(small["letters"], small["rows"], k, 10)
+    with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=10) as ix:
+        d_ans = torch.empty(want.size, dtype=torch.int64, device=cuda)
+        rep = ix.autotune(_t(small["letters"], cuda), _t(small["rows"], cuda), d_ans, want.size, tune_p=True,
+                          tune_poppy=True)
+        assert rep["best"]["ms"] > 0 and len(rep["candidates"]) >= 36
+        got = run_reads(ix, small["letters"], small["rows"], cuda)
+    assert np.array_equal(got, want)
+
+
+def test_graph_replay_matches(small, cuda):
+    import torch
+    b, k = small["built"], small["k"]
+    ox = orc.OracleIndex(b.bits, b.n_bits)
+    want = ox.search_reads(small["letters"], small["rows"], k, 10)
+    s = torch.cuda.Stream(device=cuda)
+    with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=10) as ix:
+        ix.use_graphs(True)
+        d_l, d_r = _t(small["letters"], cuda), _t(small["rows"], cuda)
+        for rep in range(3):
+            d_ans = torch.full((want.size,), -1, dtype=torch.int64, device=cuda)
+            with torch.cuda.stream(s):
+                ix.search_reads(d_l, d_r, d_ans, want.size, stream=s)
+            s.synchronize()
+            assert np.array_equal(_u64(d_ans), want), rep
+        # same buffers again: the captured graph is replayed
+        d_ans.fill_(-1)
+        ix.search_reads(d_l, d_r, d_ans, want.size, stream=s)
+        s.synchronize()
+        assert np.array_equal(_u64(d_ans), want)
+        ix.presearch(7)  # the index changed: the graph is re-captured
+        d_ans.fill_(-1)
+        ix.search_reads(d_l, d_r, d_ans, want.size, stream=s)
+        s.synchronize()
+        assert np.array_equal(_u64(d_ans), want)
+
+
+def test_l2_fetch_granularity(small, cuda):
+    b = small["built"]
+    with sg.Index.from_bits(b.bits, b.n_bits, k=31) as ix:
+        for v in (32, 64, 128):
+            ix.set_l2_fetch_granularity(v)
+        with pytest.raises(sg.SbwtError):
+            ix.set_l2_fetch_granularity(48)
+
+
+def test_many_files_one_batch(small, cuda, tmp_path):
+    b, k = small["built"], small["k"]
+    ox = orc.OracleIndex(b.bits, b.n_bits)
+    rng = wl.rng_for(77)
+    paths, wants = [], []
+    for f in range(5):
+        letters, rows = wl.mixed_reads(rng, small["genome"], 10 + f, 10, 60 + 40 * f, 0.01)
+        p = str(tmp_path / f"q{f}.fa")
+        wl.write_fasta(p, letters, rows)
+        paths.append(p)
+        wants.append(ox.search_reads(letters, rows, k, 10))
+    letters, rows, nk, file_rows = sg.read_queries_many(paths, k)
+    with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=10) as ix:
+        got = run_reads(ix, letters, rows, cuda)
+    assert np.array_equal(got, np.concatenate(wants))
