@@ -199,7 +199,7 @@ uint64_t sbwt_count_kmers(const uint64_t *row_starts, uint64_t n_rows, uint32_t 
  * shape (line layout x k-mers per thread {1,2,3,4,6,8} x threads per k-mer
  * {1,2,4} x threads per block {128,256}; with SBWT_TUNE_POPPY also the poppy
  * layouts SB 512/1024/2048 with and without shuffles; with SBWT_TUNE_P also
- * presearch depths {8,10,12,14} <= k), checks that every candidate's answers
+ * presearch depths {8,10,12,14,15} <= k), checks that every candidate's answers
  * have the same checksum, and leaves the fastest configured on the index.
  * d_answers: device scratch of n_kmers u64.  report (optional): JSON of all
  * timings (fails if report_cap is too small). */
@@ -208,6 +208,65 @@ uint64_t sbwt_count_kmers(const uint64_t *row_starts, uint64_t n_rows, uint32_t 
 int sbwt_autotune(sbwt_index *index, const uint8_t *d_letters, uint64_t n_letters, const uint64_t *d_row_starts,
                   uint64_t n_rows, uint64_t n_kmers, uint64_t *d_answers, uint32_t flags, char *report,
                   uint64_t report_cap);
+
+/* ------------------------------------------------------ learned prefilter */
+
+/* A small BF16 MLP (one-hot k-mer, 4k <= 128 inputs -> 256 ReLU -> 256 ReLU
+ * -> 1 logit, FP32 accumulation on the tensor cores) in a learned-Bloom
+ * sandwich in front of the exact search.  No reference counterpart.  A
+ * k-mer whose logit is below tau is checked against a Bloom filter over
+ * every indexed k-mer the model rejects; only a k-mer that both reject is
+ * answered "absent" without a search.  No indexed k-mer is ever reported
+ * absent, so answers equal the plain search's bit for bit. */
+typedef struct sbwt_prefilter sbwt_prefilter;
+
+typedef struct {
+    uint32_t steps;       /* Adam steps (20000) */
+    uint32_t batch;       /* batch size, a multiple of 256 (8192) */
+    float lr;             /* Adam learning rate (1e-3) */
+    uint64_t n_positive;  /* expected positives: k-mers of random index nodes, with replacement (5e7) */
+    uint64_t n_negative;  /* expected negatives: half uniform random, half positives with 1-3 substitutions (5e7) */
+    uint64_t seed;
+    float tau;            /* logit threshold (0) */
+    float bloom_fpr;      /* false-positive rate of the backup filter (0.01) */
+    uint32_t bloom_hashes; /* (3) */
+} sbwt_mlp_params;
+
+typedef struct {
+    float first_loss, final_loss;   /* mean BCE of the first and the last step */
+    float train_ms, total_ms;       /* training loop; whole call */
+    uint64_t n_train;               /* labelled candidates (labels from the exact search) */
+    double label_positive_fraction; /* share of candidates the index holds */
+    double train_accuracy;          /* on the first 4M candidates at tau */
+    uint64_t n_indexed_kmers;       /* k-mers of the index (its non-dummy nodes) */
+    uint64_t n_rejected_indexed;    /* of those, logit < tau: all inserted into the Bloom filter */
+    uint64_t bloom_bits;
+} sbwt_prefilter_stats;
+
+int sbwt_mlp_params_default(sbwt_mlp_params *params);
+/* Samples and labels the training set on the GPU, trains the MLP, builds the
+ * Bloom filter (k must be the index's; the index needs the line layout). */
+int sbwt_prefilter_train(sbwt_index *index, const sbwt_mlp_params *params, sbwt_prefilter **out);
+int sbwt_prefilter_stats_get(const sbwt_prefilter *pf, sbwt_prefilter_stats *out);
+/* The 99073 FP32 parameters: W1[256][128], b1[256], W2[256][256], b2[256], w3[256], b3. */
+int sbwt_prefilter_params(const sbwt_prefilter *pf, float *theta, uint64_t count);
+void sbwt_prefilter_free(sbwt_prefilter *pf);
+/* Logits of n k-mers (device u64 words, first letter in bits 63..62). */
+int sbwt_prefilter_logits(sbwt_prefilter *pf, const uint64_t *d_kmers, uint64_t n, float *d_logits, void *stream);
+
+/* Exact answers of a list of k-mers given as MSB-first u64 words (device). */
+int sbwt_search_kmers(sbwt_index *index, const uint64_t *d_kmers, uint64_t n, uint64_t *d_answers, void *stream);
+/* The same behind the prefilter; *n_skipped (optional, synchronizes) = k-mers
+ * answered without a search. */
+int sbwt_search_kmers_filtered(sbwt_index *index, sbwt_prefilter *pf, const uint64_t *d_kmers, uint64_t n,
+                               uint64_t *d_answers, uint64_t *n_skipped, void *stream);
+
+/* Test hooks of the training kernels: loss and gradient of one BCE step for
+ * the given parameters and batch (n a multiple of 256), and the logits of
+ * the fused inference kernel, all on device 0. */
+int sbwt_mlp_gradients(uint32_t k, const float *theta, const uint64_t *kmers, const uint8_t *labels, uint32_t n,
+                       float *loss, float *grad);
+int sbwt_mlp_logits(uint32_t k, const float *theta, const uint64_t *kmers, uint64_t n, float *logits);
 
 /* ------------------------------------------------------------ query files */
 

@@ -19,13 +19,15 @@ from ctypes import POINTER, byref, c_uint32, c_uint64, c_void_p
 import numpy as np
 
 from ._lib import (CLI_PATH, LIB_PATH, SBWT_CUM_POPPY, SBWT_LAYOUT_LINES, SBWT_LAYOUT_POPPY, SBWT_POPPY, Built,
-                   Params, Profile, Queries, SbwtError, check, lib)
+                   MlpParams, Params, PrefilterStats, Profile, Queries, SbwtError, check, lib)
 
 __all__ = [
     "Index", "Params", "SbwtError", "build_sbwt", "write_index_files", "read_queries", "format_answers",
     "count_kmers", "read_queries_many", "default_params", "SBWT_POPPY", "SBWT_CUM_POPPY", "SBWT_LAYOUT_LINES", "SBWT_LAYOUT_POPPY",
-    "LIB_PATH", "CLI_PATH", "NOT_FOUND",
+    "LIB_PATH", "CLI_PATH", "NOT_FOUND", "Prefilter", "mlp_params", "mlp_gradients", "mlp_logits", "MLP_PARAMS",
 ]
+
+MLP_PARAMS = 256 * 128 + 256 + 256 * 256 + 256 + 256 + 1  # W1, b1, W2, b2, w3, b3
 
 NOT_FOUND = 0xFFFFFFFFFFFFFFFF  # answer of an absent k-mer (printed as -1)
 
@@ -180,6 +182,19 @@ class Index:
         check(lib.sbwt_search_reads(self._h, _ptr(d_letters), int(d_letters.numel()), _ptr(d_row_starts), n_rows,
                                     _ptr(d_answers), _ptr(d_member_bits), int(n_kmers), _stream_ptr(stream)))
 
+    def search_kmers(self, d_kmers, d_answers, n=None, stream=None):
+        """Exact answers of k-mers given as MSB-first 64-bit words (device tensors)."""
+        n = int(d_kmers.numel()) if n is None else int(n)
+        check(lib.sbwt_search_kmers(self._h, _ptr(d_kmers), n, _ptr(d_answers), _stream_ptr(stream)))
+
+    def search_kmers_filtered(self, prefilter, d_kmers, d_answers, n=None, stream=None):
+        """The same behind the learned prefilter; returns the number of k-mers answered without a search."""
+        n = int(d_kmers.numel()) if n is None else int(n)
+        sk = c_uint64()
+        check(lib.sbwt_search_kmers_filtered(self._h, prefilter._h, _ptr(d_kmers), n, _ptr(d_answers), byref(sk),
+                                             _stream_ptr(stream)))
+        return sk.value
+
     def search_reads_host(self, letters, row_starts, answers=None):
         """Host reads -> host answers (numpy), streamed through the GPU."""
         letters = np.ascontiguousarray(letters, dtype=np.uint8) if isinstance(letters, np.ndarray) else letters
@@ -195,6 +210,84 @@ class Index:
         n_letters = letters.size if isinstance(letters, np.ndarray) else letters.numel()
         check(lib.sbwt_search_reads_host(self._h, _ptr(letters), int(n_letters), _ptr(rs), n_rows, _ptr(answers), nk))
         return answers[:nk] if isinstance(answers, np.ndarray) else answers
+
+
+# ------------------------------------------------------- learned prefilter
+
+def mlp_params(**kw):
+    """``sbwt_mlp_params`` with the defaults of the prefilter configuration, overridden by ``kw``."""
+    p = MlpParams()
+    check(lib.sbwt_mlp_params_default(byref(p)))
+    for key, val in kw.items():
+        if not hasattr(p, key):
+            raise TypeError(f"unknown parameter {key}")
+        setattr(p, key, val)
+    return p
+
+
+class Prefilter:
+    """A trained MLP + backup Bloom filter (``sbwt_prefilter*``)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def train(cls, index, params=None, **kw):
+        p = params if params is not None else mlp_params(**kw)
+        h = c_void_p()
+        check(lib.sbwt_prefilter_train(index._h, byref(p), byref(h)))
+        return cls(h)
+
+    def stats(self):
+        st = PrefilterStats()
+        check(lib.sbwt_prefilter_stats_get(self._h, byref(st)))
+        return {name: getattr(st, name) for name, _ in PrefilterStats._fields_}
+
+    def params(self):
+        th = np.empty(MLP_PARAMS, dtype=np.float32)
+        check(lib.sbwt_prefilter_params(self._h, _ptr(th), MLP_PARAMS))
+        return th
+
+    def logits(self, d_kmers, d_logits, n=None, stream=None):
+        n = int(d_kmers.numel()) if n is None else int(n)
+        check(lib.sbwt_prefilter_logits(self._h, _ptr(d_kmers), n, _ptr(d_logits), _stream_ptr(stream)))
+
+    def close(self):
+        if self._h:
+            lib.sbwt_prefilter_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def mlp_gradients(k, theta, kmers, labels):
+    """Loss and gradient of one BCE step of the GPU training kernels (test hook)."""
+    th = np.ascontiguousarray(theta, dtype=np.float32)
+    km = np.ascontiguousarray(kmers, dtype=np.uint64)
+    lb = np.ascontiguousarray(labels, dtype=np.uint8)
+    grad = np.empty(MLP_PARAMS, dtype=np.float32)
+    loss = ctypes.c_float()
+    check(lib.sbwt_mlp_gradients(int(k), _ptr(th), _ptr(km), _ptr(lb), km.size, byref(loss), _ptr(grad)))
+    return loss.value, grad
+
+
+def mlp_logits(k, theta, kmers):
+    """Logits of the fused tensor-core inference kernel (test hook)."""
+    th = np.ascontiguousarray(theta, dtype=np.float32)
+    km = np.ascontiguousarray(kmers, dtype=np.uint64)
+    out = np.empty(max(km.size, 1), dtype=np.float32)
+    check(lib.sbwt_mlp_logits(int(k), _ptr(th), _ptr(km), km.size, _ptr(out)))
+    return out[: km.size]
 
 
 # ------------------------------------------------------------------ builder

@@ -72,6 +72,39 @@ class Profile(ctypes.Structure):
     ]
 
 
+class MlpParams(ctypes.Structure):
+    """Mirror of ``sbwt_mlp_params``."""
+
+    _fields_ = [
+        ("steps", c_uint32),
+        ("batch", c_uint32),
+        ("lr", ctypes.c_float),
+        ("n_positive", c_uint64),
+        ("n_negative", c_uint64),
+        ("seed", c_uint64),
+        ("tau", ctypes.c_float),
+        ("bloom_fpr", ctypes.c_float),
+        ("bloom_hashes", c_uint32),
+    ]
+
+
+class PrefilterStats(ctypes.Structure):
+    """Mirror of ``sbwt_prefilter_stats``."""
+
+    _fields_ = [
+        ("first_loss", ctypes.c_float),
+        ("final_loss", ctypes.c_float),
+        ("train_ms", ctypes.c_float),
+        ("total_ms", ctypes.c_float),
+        ("n_train", c_uint64),
+        ("label_positive_fraction", ctypes.c_double),
+        ("train_accuracy", ctypes.c_double),
+        ("n_indexed_kmers", c_uint64),
+        ("n_rejected_indexed", c_uint64),
+        ("bloom_bits", c_uint64),
+    ]
+
+
 # name -> (restype, argtypes): every symbol include/sbwt_gpu.h declares
 SIGNATURES = {
     "sbwt_params_default": (c_int, [POINTER(Params)]),
@@ -94,6 +127,18 @@ SIGNATURES = {
     "sbwt_use_graphs": (c_int, [c_void_p, c_int]),
     "sbwt_set_l2_fetch_granularity": (c_int, [c_void_p, c_uint32]),
     "sbwt_profile_read": (c_int, [c_void_p, POINTER(Profile)]),
+    "sbwt_mlp_params_default": (c_int, [POINTER(MlpParams)]),
+    "sbwt_prefilter_train": (c_int, [c_void_p, POINTER(MlpParams), POINTER(c_void_p)]),
+    "sbwt_prefilter_stats_get": (c_int, [c_void_p, POINTER(PrefilterStats)]),
+    "sbwt_prefilter_params": (c_int, [c_void_p, c_void_p, c_uint64]),
+    "sbwt_prefilter_free": (None, [c_void_p]),
+    "sbwt_prefilter_logits": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_void_p]),
+    "sbwt_search_kmers": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_void_p]),
+    "sbwt_search_kmers_filtered": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_void_p, POINTER(c_uint64),
+                                           c_void_p]),
+    "sbwt_mlp_gradients": (c_int, [c_uint32, c_void_p, c_void_p, c_void_p, c_uint32, POINTER(ctypes.c_float),
+                                   c_void_p]),
+    "sbwt_mlp_logits": (c_int, [c_uint32, c_void_p, c_void_p, c_uint64, c_void_p]),
     "sbwt_queries_read": (c_int, [c_char_p, c_uint32, POINTER(Queries)]),
     "sbwt_queries_read_many": (c_int, [POINTER(c_char_p), c_int, c_uint32, POINTER(Queries), c_void_p]),
     "sbwt_autotune": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_uint64, c_void_p, c_uint32, c_void_p,

@@ -52,6 +52,8 @@ int grow_host(T *&p, size_t &cap, size_t need) {
 }
 
 template int grow<uint8_t>(uint8_t *&, size_t &, size_t);
+template int grow<uint32_t>(uint32_t *&, size_t &, size_t);
+template int grow<unsigned long long>(unsigned long long *&, size_t &, size_t);
 template int grow<uint64_t>(uint64_t *&, size_t &, size_t);
 template int grow_host<uint8_t>(uint8_t *&, size_t &, size_t);
 template int grow_host<uint64_t>(uint64_t *&, size_t &, size_t);
@@ -78,9 +80,11 @@ int validate_params(const sbwt_params *p) {
 void apply_shape(sbwt_index *ix, const sbwt_params *p) {
     sbwt::KernelShape &sh = ix->shape;
     sh.layout = p->layout == SBWT_LAYOUT_POPPY ? SBWT_LAYOUT_POPPY : SBWT_LAYOUT_LINES;
-    sh.kpt = p->kmers_per_thread ? p->kmers_per_thread : 4;
+    // defaults from the autotuner on the large workload (1 k-mer per thread,
+    // 128-thread blocks: occupancy beats register-resident k-mer slots)
+    sh.kpt = p->kmers_per_thread ? p->kmers_per_thread : 1;
     sh.tpk = p->threads_per_kmer ? p->threads_per_kmer : 1;
-    sh.tpb = p->threads_per_block ? std::min<u32>(p->threads_per_block, 256u) : 256u;
+    sh.tpb = p->threads_per_block ? std::min<u32>(p->threads_per_block, 256u) : 128u;
     sh.sb = p->bits_in_superblock;
     sh.kind = p->rank_structure;
     sh.shuffles = p->with_shuffles;

@@ -8,7 +8,7 @@
 // fastest: line layout x k-mers per thread {1,2,3,4,6,8} x threads per k-mer
 // {1,2,4} x threads per block {128,256}; optionally the reference's poppy
 // layouts (SB 512/1024/2048, with and without the cooperative "shuffles"
-// rank); and optionally presearch depths p in {8,10,12,14} (p <= k).  Every
+// rank); and optionally presearch depths p in {8,10,12,14,15} (p <= k).  Every
 // candidate's answers are reduced to an order-sensitive checksum, and all
 // checksums must agree: the sweep doubles as a bit-exactness check across
 // shapes at full size.
@@ -147,7 +147,7 @@ extern "C" int sbwt_autotune(sbwt_index *ix, const uint8_t *d_letters, uint64_t 
         std::sort(ranked.begin(), ranked.end(), [](const Cand &a, const Cand &b) { return a.ms < b.ms; });
         Cand best = ranked.front();
         if (flags & 2u) {
-            for (u32 p : {8u, 10u, 12u, 14u}) {
+            for (u32 p : {8u, 10u, 12u, 14u, 15u}) {
                 if (p > ix->k || p == best.p) continue;
                 Cand c = best;
                 c.p = p;

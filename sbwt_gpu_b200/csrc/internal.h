@@ -38,13 +38,22 @@ struct SearchArgs {
     u64 n_kmers;
     unsigned long long *counter;  // work-stealing cursor (zeroed before launch)
     u32 chunk;                    // k-mers per grab
+    // k-mer list mode: k-mer j is kmer_list[j] (MSB-first word)
+    const u64 *kmer_list;
+    // learned prefilter: skip k-mer j if logits[j] < tau and the Bloom filter rejects it
+    const float *logits;
+    float tau;
+    const uint32_t *bloom_bits;
+    u64 bloom_mask;
+    u32 bloom_hashes;
+    unsigned long long *skipped;
 };
 
 struct KernelShape {
     int layout = SBWT_LAYOUT_LINES;
-    u32 kpt = 2;   // k-mer slots per thread
+    u32 kpt = 1;   // k-mer slots per thread
     u32 tpk = 1;   // lanes per k-mer
-    u32 tpb = 256; // threads per block
+    u32 tpb = 128; // threads per block
     u32 sb = 1024;
     int kind = SBWT_POPPY;
     int shuffles = 0;

@@ -94,7 +94,7 @@ int run_presearch(sbwt_index *ix, uint32_t p, cudaStream_t s) {
     ix->p = 0;
     if (p == 0) return 0;  // search without presearch (parameters.hpp:555, search_kernel.hpp:79-81)
     if (p > ix->k) return set_error("presearch depth p=%u exceeds k=%u", p, ix->k);
-    if (p > 15) return set_error("presearch depth p=%u is larger than 15 (a 4^p table)", p);
+    if (p > 16) return set_error("presearch depth p=%u is larger than 16 (a 4^p-entry table)", p);
     ix->pre64 = ix->n >= (1ull << 32);
     const size_t esz = ix->pre64 ? sizeof(ulonglong2) : sizeof(uint2);
     const u64 count = 1ull << (2 * p);

@@ -27,6 +27,7 @@
 
 #include "device.cuh"
 #include "internal.h"
+#include "mlp_kernels.cuh"
 #include "rank.cuh"
 
 namespace sbwt {
@@ -66,7 +67,9 @@ __global__ void __launch_bounds__(256, MinBlocks<KPT>::value) search_kernel(cons
     for (int s = 0; s < KPT; s++) { I[s] = kDone; kmer[s] = 0; J[s] = 0; L[s] = 0; R_[s] = 0; }
 
     // k-mers of this launch; in read mode never more than the row table holds
-    const u64 n_eff = a.positions ? a.n_kmers : min(a.n_kmers, a.kstart[a.n_rows]);
+    const bool read_mode = !a.positions && !a.kmer_list;
+    const u64 n_eff = read_mode ? min(a.n_kmers, a.kstart[a.n_rows]) : a.n_kmers;
+    const mlp::Bloom bloom{a.bloom_bits, a.bloom_mask, a.bloom_hashes};
     u64 q_next = 0, q_end = 0, row = 0;
     bool more = true;
 
@@ -85,26 +88,37 @@ __global__ void __launch_bounds__(256, MinBlocks<KPT>::value) search_kernel(cons
                     if (base >= n_eff) { more = false; break; }
                     q_next = base;
                     q_end = min((u64)base + a.chunk, n_eff);
-                    if (!a.positions) row = a.chunk_row[base / a.chunk];
+                    if (read_mode) row = a.chunk_row[base / a.chunk];
                 }
                 const u32 take = (u32)min((u64)__popc(m), q_end - q_next);
                 const u32 rk_ = __popc(m & lead_lt);
                 const bool got = need && rk_ < take;
                 u64 rr = row;
+                bool skip = false;
                 if (got) {
                     const u64 j = q_next + rk_;
-                    u64 pos;
-                    if (a.positions) {
-                        pos = a.positions[j];
+                    u64 km;
+                    if (a.kmer_list) {
+                        km = a.kmer_list[j];
                     } else {
-                        while (rr + 1 < a.n_rows && a.kstart[rr + 1] <= j) rr++;
-                        pos = a.row_starts[rr] + (j - a.kstart[rr]);
+                        u64 pos;
+                        if (a.positions) {
+                            pos = a.positions[j];
+                        } else {
+                            while (rr + 1 < a.n_rows && a.kstart[rr + 1] <= j) rr++;
+                            pos = a.row_starts[rr] + (j - a.kstart[rr]);
+                        }
+                        pos = min(pos, a.max_pos);  // a bad offset reads garbage, never out of bounds
+                        const u64 b = pos << 1;  // search_kernel.hpp:66-68
+                        const u64 w0 = a.words[b >> 6], w1 = a.words[(b >> 6) + 1];
+                        const u32 sh = (u32)(b & 63u);
+                        km = (w0 << sh) | (shr_clamp(w1, 63u - sh) >> 1);
                     }
-                    pos = min(pos, a.max_pos);  // a bad offset reads garbage, never out of bounds
-                    const u64 b = pos << 1;  // search_kernel.hpp:66-68
-                    const u64 w0 = a.words[b >> 6], w1 = a.words[(b >> 6) + 1];
-                    const u32 sh = (u32)(b & 63u);
-                    const u64 km = (w0 << sh) | (shr_clamp(w1, 63u - sh) >> 1);
+                    // learned-Bloom sandwich: answered "absent" only if both reject
+                    if (a.logits && __ldg(a.logits + j) < a.tau && !bloom.probe(mlp::kmer_key(km, k))) {
+                        skip = true;
+                        if (sub == 0) a.answers[j] = ~0ull;
+                    }
                     kmer[s] = km;
                     J[s] = j;
                     if (p) {
@@ -115,9 +129,13 @@ __global__ void __launch_bounds__(256, MinBlocks<KPT>::value) search_kernel(cons
                         L[s] = 0;
                         R_[s] = rootR;
                     }
-                    I[s] = p;
+                    I[s] = skip ? kDone : p;
                 }
-                if (!a.positions) {
+                if (a.skipped) {
+                    const u32 sk = __ballot_sync(kFull, skip && sub == 0);
+                    if (lane == 0 && sk) atomicAdd(a.skipped, (unsigned long long)__popc(sk));
+                }
+                if (read_mode) {
                     const u32 lastm = __ballot_sync(kFull, got && sub == 0 && rk_ == take - 1u);
                     row = __shfl_sync(kFull, rr, __ffs(lastm) - 1);
                 }

@@ -1,0 +1,121 @@
+"""The learned prefilter: tensor-core kernels vs the FP32 oracle, and the
+sandwich guarantees (no indexed k-mer reported absent, answers identical to
+the plain search).  Needs a B200.
+
+Tolerances: the GPU and the oracle round to BF16 at the same points and
+differ only in FP32 accumulation order, so a value near a BF16 rounding tie
+can land one BF16 step (2^-8 relative) apart.  Logits must agree within
+2e-2 absolute + 2e-2 relative; every gradient tensor within 2e-2 of the
+oracle's in relative L2 norm.
+"""
+import numpy as np
+import pytest
+
+import mlp_oracle as mo
+import oracle as orc
+import sbwt_gpu_b200 as sg
+from sbwt_gpu_b200 import workloads as wl
+
+pytestmark = pytest.mark.gpu
+
+
+def _rand_kmers(rng, n, k):
+    mask = np.uint64(((1 << (2 * k)) - 1) << (64 - 2 * k)) if k < 32 else np.uint64(0xFFFFFFFFFFFFFFFF)
+    return rng.integers(0, 2**63, size=n, dtype=np.int64).astype(np.uint64) * np.uint64(2) & mask
+
+
+@pytest.mark.parametrize("k", [31, 15, 32])
+def test_fused_inference_matches_oracle(cuda, k):
+    rng = np.random.default_rng(k)
+    theta = mo.init_like(seed=k, k=k)
+    kmers = _rand_kmers(rng, 1000, k)  # not a multiple of the 128-row tile
+    got = sg.mlp_logits(k, theta, kmers)
+    want, _ = mo.forward(theta, kmers, k)
+    assert np.allclose(got, want, rtol=2e-2, atol=2e-2), np.abs(got - want).max()
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.parametrize("n", [256, 2048])
+def test_training_gradients_match_oracle(cuda, n):
+    rng = np.random.default_rng(n)
+    k = 31
+    theta = mo.init_like(seed=n, k=k)
+    kmers = _rand_kmers(rng, n, k)
+    labels = (rng.random(n) < 0.4).astype(np.uint8)
+    loss, g = sg.mlp_gradients(k, theta, kmers, labels)
+    wl_, wg = mo.loss_and_grad(theta, kmers, labels, k)
+    assert abs(loss - wl_) < 1e-3 * max(1.0, abs(wl_))
+    for name, a, b in [("W1", 0, 32768), ("b1", 32768, 33024), ("W2", 33024, 98560), ("b2", 98560, 98816),
+                       ("w3", 98816, 99072), ("b3", 99072, 99073)]:
+        assert _rel(g[a:b], wg[a:b]) < 2e-2, (name, _rel(g[a:b], wg[a:b]))
+    assert not g[0:32768].reshape(256, 128)[:, 4 * k:].any()  # padded inputs get no gradient
+
+
+@pytest.fixture(scope="module")
+def trained(cuda):
+    import torch
+    rng = wl.rng_for(4040)
+    k = 31
+    genome = wl.random_bases(rng, 60_000)
+    built = sg.build_sbwt([genome.tobytes()], k)
+    ix = sg.Index.from_bits(built.bits, built.n_bits, k=k, k_presearch=10)
+    pf = sg.Prefilter.train(ix, steps=400, batch=2048, n_positive=400_000, n_negative=400_000, seed=9)
+    yield {"ix": ix, "pf": pf, "genome": genome, "built": built, "k": k}
+    pf.close()
+    ix.close()
+
+
+def test_training_reduces_loss(trained):
+    st = trained["pf"].stats()
+    assert st["final_loss"] < st["first_loss"]
+    assert st["train_accuracy"] > 0.75
+    assert 0.3 < st["label_positive_fraction"] < 0.7
+    assert st["n_indexed_kmers"] == trained["built"].n_kmers
+    assert st["bloom_bits"] >= 1024
+
+
+def test_sandwich_is_bit_exact_and_never_drops_an_indexed_kmer(trained, cuda):
+    import torch
+    ix, pf, k = trained["ix"], trained["pf"], trained["k"]
+    rng = wl.rng_for(5)
+    letters, rows = wl.kmer_queries(rng, trained["genome"], 20_000, k, neg_frac=0.9)
+    kmers = orc.extract_kmers(letters, rows, k)
+    d_k = torch.from_numpy(kmers.view(np.int64)).to(cuda)
+    plain = torch.empty_like(d_k)
+    filt = torch.full_like(d_k, -5)
+    ix.search_kmers(d_k, plain)
+    skipped = ix.search_kmers_filtered(pf, d_k, filt)
+    torch.cuda.synchronize()
+    p, f = plain.cpu().numpy().view(np.uint64), filt.cpu().numpy().view(np.uint64)
+    assert np.array_equal(p, f)
+    ox = orc.OracleIndex(trained["built"].bits, trained["built"].n_bits)
+    words = np.append(kmers, np.uint64(0))  # one padding word after the last k-mer
+    assert np.array_equal(p, ox.search_positions(words, np.arange(kmers.size, dtype=np.uint64) * np.uint64(32), k, 10))
+    assert skipped > 0
+    # every indexed k-mer passes the sandwich (false-absent = 0)
+    keys, dk, _ = orc.independent_sbwt([trained["genome"].tobytes()], k)
+    g = trained["genome"]
+    all_rows = np.array([0, g.size], dtype=np.uint64)
+    all_kmers = orc.extract_kmers(g, all_rows, k)
+    d_all = torch.from_numpy(all_kmers.view(np.int64)).to(cuda)
+    out = torch.empty_like(d_all)
+    ix.search_kmers_filtered(pf, d_all, out)
+    torch.cuda.synchronize()
+    assert (out.cpu().numpy().view(np.uint64) != orc.NOT_FOUND).all()
+
+
+def test_prefilter_logits_api(trained, cuda):
+    import torch
+    pf, k = trained["pf"], trained["k"]
+    theta = pf.params()
+    rng = np.random.default_rng(3)
+    kmers = _rand_kmers(rng, 777, k)
+    d_k = torch.from_numpy(kmers.view(np.int64)).to(cuda)
+    d_l = torch.empty(777, dtype=torch.float32, device=cuda)
+    pf.logits(d_k, d_l)
+    torch.cuda.synchronize()
+    want, _ = mo.forward(theta, kmers, k)
+    assert np.allclose(d_l.cpu().numpy(), want, rtol=2e-2, atol=2e-2)
