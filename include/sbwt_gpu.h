@@ -53,7 +53,8 @@ typedef struct {
     uint32_t threads_per_block;  /* 0 = engine default (parameters.hpp:51) */
     int32_t device;              /* CUDA device ordinal (the reference uses 0, parameters.hpp:81) */
     int32_t layout;              /* SBWT_LAYOUT_LINES | SBWT_LAYOUT_POPPY */
-    uint32_t kmers_per_thread;   /* search kernel: k-mer slots per thread, 1..8 (0 = default) */
+    uint32_t kmers_per_thread;   /* search kernel: 0 = one k-mer per lane fed from a per-warp queue
+                                    (default); 1,2,3,4,6,8 = k-mer slots held in registers */
     uint32_t threads_per_kmer;   /* search kernel: lanes sharing one k-mer, 1|2|4 (0 = default) */
 } sbwt_params;
 
@@ -108,8 +109,12 @@ int sbwt_presearch_export(const sbwt_index *index, uint64_t *node_lefts, uint64_
 int sbwt_rank_export(sbwt_index *index, uint32_t bits_in_superblock, int32_t rank_structure, int c,
                      uint64_t *L0, uint64_t l0_words, uint64_t *L12, uint64_t l12_words);
 
+/* Pass for an unsigned sbwt_configure argument to leave it unchanged. */
+#define SBWT_KEEP 0xFFFFFFFFu
+
 /* Selects the search layout / kernel shape for later searches (building the
- * poppy structures if needed).  No reference counterpart: the reference
+ * poppy structures if needed); kmers_per_thread, threads_per_kmer and
+ * threads_per_block take SBWT_KEEP or 0 ... as sbwt_params documents.  No reference counterpart: the reference
  * picks these by template switch (include/epicseq/search_caller.hpp:81-209). */
 int sbwt_configure(sbwt_index *index, int32_t layout, uint32_t bits_in_superblock, int32_t rank_structure,
                    int32_t with_shuffles, uint32_t kmers_per_thread, uint32_t threads_per_kmer,

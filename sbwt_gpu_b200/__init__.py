@@ -30,6 +30,7 @@ __all__ = [
 MLP_PARAMS = 256 * 128 + 256 + 256 * 256 + 256 + 256 + 1  # W1, b1, W2, b2, w3, b3
 
 NOT_FOUND = 0xFFFFFFFFFFFFFFFF  # answer of an absent k-mer (printed as -1)
+SBWT_KEEP = 0xFFFFFFFF  # sbwt_configure: leave the argument unchanged
 
 
 def default_params(**kw):
@@ -137,7 +138,8 @@ class Index:
         return L0, L12
 
     def configure(self, layout=SBWT_LAYOUT_LINES, bits_in_superblock=1024, rank_structure=SBWT_POPPY,
-                  with_shuffles=0, kmers_per_thread=0, threads_per_kmer=0, threads_per_block=0):
+                  with_shuffles=0, kmers_per_thread=SBWT_KEEP, threads_per_kmer=SBWT_KEEP,
+                  threads_per_block=SBWT_KEEP):
         check(lib.sbwt_configure(self._h, layout, bits_in_superblock, rank_structure, int(with_shuffles),
                                  kmers_per_thread, threads_per_kmer, threads_per_block))
 

@@ -82,7 +82,7 @@ void apply_shape(sbwt_index *ix, const sbwt_params *p) {
     sh.layout = p->layout == SBWT_LAYOUT_POPPY ? SBWT_LAYOUT_POPPY : SBWT_LAYOUT_LINES;
     // defaults from the autotuner on the large workload (1 k-mer per thread,
     // 128-thread blocks: occupancy beats register-resident k-mer slots)
-    sh.kpt = p->kmers_per_thread ? p->kmers_per_thread : 1;
+    sh.kpt = p->kmers_per_thread;  // 0: the queue-fed single-slot kernel
     sh.tpk = p->threads_per_kmer ? p->threads_per_kmer : 1;
     sh.tpb = p->threads_per_block ? std::min<u32>(p->threads_per_block, 256u) : 128u;
     sh.sb = p->bits_in_superblock;
@@ -338,18 +338,20 @@ extern "C" int sbwt_configure(sbwt_index *ix, int32_t layout, uint32_t sb, int32
     } else {
         return set_error("unknown layout %d", layout);
     }
-    if (tpb && (tpb % 32 || tpb > 256)) return set_error("threads_per_block must be a multiple of 32 up to 256");
-    if (kpt && !(kpt == 1 || kpt == 2 || kpt == 3 || kpt == 4 || kpt == 6 || kpt == 8))
-        return set_error("kmers_per_thread must be 1, 2, 3, 4, 6 or 8");
-    if (tpk && !(tpk == 1 || tpk == 2 || tpk == 4)) return set_error("threads_per_kmer must be 1, 2 or 4");
+    if (tpb != SBWT_KEEP && tpb && (tpb % 32 || tpb > 256))
+        return set_error("threads_per_block must be a multiple of 32 up to 256");
+    if (kpt != SBWT_KEEP && !(kpt == 0 || kpt == 1 || kpt == 2 || kpt == 3 || kpt == 4 || kpt == 6 || kpt == 8))
+        return set_error("kmers_per_thread must be 0 (queue-fed), 1, 2, 3, 4, 6 or 8");
+    if (tpk != SBWT_KEEP && tpk && !(tpk == 1 || tpk == 2 || tpk == 4))
+        return set_error("threads_per_kmer must be 1, 2 or 4");
     KernelShape &sh = ix->shape;
     sh.layout = layout;
     sh.sb = sb;
     sh.kind = kind;
     sh.shuffles = shuffles;
-    if (kpt) sh.kpt = kpt;
-    if (tpk) sh.tpk = tpk;
-    if (tpb) sh.tpb = tpb;
+    if (kpt != SBWT_KEEP) sh.kpt = kpt;
+    if (tpk != SBWT_KEEP && tpk) sh.tpk = tpk;
+    if (tpb != SBWT_KEEP && tpb) sh.tpb = tpb;
     return 0;
 }
 

@@ -5,7 +5,8 @@
 //
 // On a caller-supplied sample batch (device letters + row starts) the tuner
 // times sbwt_search_reads for each candidate launch shape and keeps the
-// fastest: line layout x k-mers per thread {1,2,3,4,6,8} x threads per k-mer
+// fastest: the queue-fed single-slot kernel and the line layout x k-mers per
+// thread {1,2,3,4,6,8} x threads per k-mer
 // {1,2,4} x threads per block {128,256}; optionally the reference's poppy
 // layouts (SB 512/1024/2048, with and without the cooperative "shuffles"
 // rank); and optionally presearch depths p in {8,10,12,14,15} (p <= k).  Every
@@ -130,15 +131,20 @@ extern "C" int sbwt_autotune(sbwt_index *ix, const uint8_t *d_letters, uint64_t 
         }
         const u32 p0 = saved_p;
         std::vector<Cand> stage1;
-        if (ix->lines_ok)
+        if (ix->lines_ok) {
+            stage1.push_back(Cand{SBWT_LAYOUT_LINES, 0, 1, 128, 1024, 0, p0, 0, 0});  // queue-fed single slot
             for (u32 tpb : {128u, 256u})
                 for (u32 tpk : {1u, 2u, 4u})
                     for (u32 kpt : {1u, 2u, 3u, 4u, 6u, 8u}) stage1.push_back(Cand{SBWT_LAYOUT_LINES, kpt, tpk, tpb, 1024, 0, p0, 0, 0});
+        }
         if ((flags & 4u) || !ix->lines_ok)
             for (u32 sb : {512u, 1024u, 2048u})
                 for (int sh : {0, 1}) {
                     if (sh && sb == 512) continue;
-                    for (u32 kpt : {1u, 2u}) stage1.push_back(Cand{SBWT_LAYOUT_POPPY, kpt, 1, 256, sb, sh, p0, 0, 0});
+                    for (u32 kpt : {0u, 1u, 2u}) {
+                        if (kpt == 0 && sh) continue;
+                        stage1.push_back(Cand{SBWT_LAYOUT_POPPY, kpt, 1, kpt == 0 ? 128u : 256u, sb, sh, p0, 0, 0});
+                    }
                 }
         for (Cand &c : stage1)
             if ((rc = measure(c)) != 0) break;

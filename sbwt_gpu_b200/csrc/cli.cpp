@@ -65,7 +65,7 @@ int parse(int argc, char **argv, Options &o) {
     const std::regex k_re{"^--k=([3-9]|([1-2][0-9])|3[0-2])$"};
     const std::regex kp_re{"^--k-presearch=([1-9]|(1[0-5]))$"};
     const std::regex tpb_re{"^--threads-per-block=([0-9][0-9][0-9]?[0-9]?)$"};
-    const std::regex kpt_re{"^--kmers-per-thread=([1-8])$"};
+    const std::regex kpt_re{"^--kmers-per-thread=([0-8])$"};
     const std::regex tpk_re{"^--threads-per-kmer=(1|2|4)$"};
     std::smatch m;
     for (int i = 1; i < argc; i++) {
@@ -92,7 +92,7 @@ int parse(int argc, char **argv, Options &o) {
         else if (std::regex_match(s, m, tpk_re)) o.p.threads_per_kmer = (uint32_t)std::stoul(m[1]);
         else if (std::regex_match(s, m, tpb_re)) {
             const unsigned v = (unsigned)std::stoul(m[1]);
-            if (v < 32 || v > 256 || v % 32)  // parameters.hpp:223-231 (our kernels take at most 256)
+            if (v < 32 || v > 256 || v % 32)  // parameters.hpp:202-212 (our kernels take at most 256)
                 std::fprintf(stderr, "Number of threads per block should have been at least 32 and at most 256. "
                                      "We use now the default.\n");
             else
@@ -106,7 +106,7 @@ int parse(int argc, char **argv, Options &o) {
         else std::fprintf(stderr, "Unknown argument %s ignored.\n", s.c_str());
     }
     if (o.with_presearch) {
-        if (o.p.k_presearch < 5 || o.p.k_presearch > 13) {  // parameters.hpp:244-252
+        if (o.p.k_presearch < 5 || o.p.k_presearch > 13) {  // parameters.hpp:253-265
             std::fprintf(stderr, "The value of the prefix of k-mers to be presearched must be at least 5 and at most 13.\n");
             o.p.k_presearch = 12;
         }

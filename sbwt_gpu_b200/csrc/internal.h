@@ -51,7 +51,7 @@ struct SearchArgs {
 
 struct KernelShape {
     int layout = SBWT_LAYOUT_LINES;
-    u32 kpt = 1;   // k-mer slots per thread
+    u32 kpt = 0;   // k-mer slots per thread (0: the queue-fed single-slot kernel)
     u32 tpk = 1;   // lanes per k-mer
     u32 tpb = 128; // threads per block
     u32 sb = 1024;

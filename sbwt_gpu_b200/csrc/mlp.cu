@@ -505,6 +505,14 @@ int gemm_tn(const bf16 *A, const bf16 *B, float *D, u32 M, u32 N, u32 K, u32 spl
     splits = (K + kps - 1) / kps;
     const dim3 grid(M / 128, 1, splits);
     const int atomic = splits > 1;
+    static bool attr_set = false;  // 48 KiB of dynamic shared memory needs the opt-in
+    if (!attr_set) {
+        SBWT_CHECK_CUDA(cudaFuncSetAttribute(gemm_tn_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             128 * 64 * 2 + 256 * 64 * 2));
+        SBWT_CHECK_CUDA(cudaFuncSetAttribute(gemm_tn_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             128 * 64 * 2 + 128 * 64 * 2));
+        attr_set = true;
+    }
     if (atomic) SBWT_CHECK_CUDA(cudaMemsetAsync(D, 0, (size_t)M * N * sizeof(float), s));
     if (N == 256) {
         const u32 smem = 128 * 64 * 2 + 256 * 64 * 2;

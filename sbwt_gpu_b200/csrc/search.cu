@@ -175,6 +175,158 @@ __global__ void __launch_bounds__(256, MinBlocks<KPT>::value) search_kernel(cons
     }
 }
 
+
+// ------------------------------------------------- queue-fed single-slot form
+//
+// One k-mer per lane, with the per-k-mer set-up done cooperatively: when its
+// queue in shared memory runs low, a whole warp takes the next 32 indices of
+// its chunk at once (position, k-mer, presearch entry, prefilter check, all
+// 32 lanes active) and enqueues the k-mers that still need steps; a lane
+// whose k-mer finishes pops the next entry (ballot + popc).  K-mers settled
+// by the presearch entry alone (empty interval, or p = k) are answered
+// during the fill and never enqueued.
+
+constexpr u32 kQueue = 64;         // entries per warp (power of two)
+constexpr u32 kQueueWarps = 4;     // 128-thread blocks
+
+struct QEntry {
+    u64 kmer, j;
+    u32 l, r;
+};
+
+template <class R>
+__global__ void __launch_bounds__(128) search_queue_kernel(const R rk, const SearchArgs a) {
+    static_assert(sizeof(typename R::IT) == 4, "the queue form serves 32-bit intervals");
+    __shared__ QEntry queue[kQueueWarps][kQueue];
+    using PT = uint2;
+    const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const u32 lt = (1u << lane) - 1u;
+    const u32 k = a.k, p = a.p;
+    const u32 C0 = (u32)a.C[0], C1 = (u32)a.C[1], C2 = (u32)a.C[2], C3 = (u32)a.C[3];
+    const u32 rootR = (u32)(a.C[4] - 1ull);
+    const PT *pre = reinterpret_cast<const PT *>(a.pre);
+    const bool read_mode = !a.positions && !a.kmer_list;
+    const u64 n_eff = read_mode ? min(a.n_kmers, a.kstart[a.n_rows]) : a.n_kmers;
+    const mlp::Bloom bloom{a.bloom_bits, a.bloom_mask, a.bloom_hashes};
+    QEntry *q = queue[warp];
+
+    // warp-uniform queue / chunk state
+    u32 head = 0, tail = 0;
+    u64 c_next = 0, c_end = 0, row = 0;
+    bool more = true;
+    // lane state
+    u64 kmer = 0, J = 0;
+    u32 L = 0, Rr = 0, I = kDone;
+
+    for (;;) {
+        // ---- cooperative fill
+        if (more && tail - head < 32u) {
+            if (c_next >= c_end) {
+                unsigned long long base = 0;
+                if (lane == 0) base = atomicAdd(a.counter, (unsigned long long)a.chunk);
+                base = __shfl_sync(kFull, base, 0);
+                if (base >= n_eff) {
+                    more = false;
+                } else {
+                    c_next = base;
+                    c_end = min((u64)base + a.chunk, n_eff);
+                    if (read_mode) row = a.chunk_row[base / a.chunk];
+                }
+            }
+            if (more) {
+                const u64 j = c_next + lane;
+                const bool valid = j < c_end;
+                const u32 cnt = (u32)min((u64)32, c_end - c_next);
+                u64 km = 0, rr = row;
+                u32 l = 0, r = 0;
+                bool enq = false;
+                if (valid) {
+                    if (a.kmer_list) {
+                        km = a.kmer_list[j];
+                    } else {
+                        u64 pos;
+                        if (a.positions) {
+                            pos = a.positions[j];
+                        } else {
+                            while (rr + 1 < a.n_rows && a.kstart[rr + 1] <= j) rr++;
+                            pos = a.row_starts[rr] + (j - a.kstart[rr]);
+                        }
+                        pos = min(pos, a.max_pos);
+                        const u64 b = pos << 1;  // search_kernel.hpp:66-68
+                        const u64 w0 = a.words[b >> 6], w1 = a.words[(b >> 6) + 1];
+                        const u32 sh = (u32)(b & 63u);
+                        km = (w0 << sh) | (shr_clamp(w1, 63u - sh) >> 1);
+                    }
+                    bool skip = false;
+                    if (a.logits && __ldg(a.logits + j) < a.tau && !bloom.probe(mlp::kmer_key(km, k))) skip = true;
+                    if (!skip) {
+                        if (p) {
+                            const PT e = pre[km >> (64u - 2u * p)];
+                            l = e.x;
+                            r = e.y;
+                        } else {
+                            l = 0;
+                            r = rootR;
+                        }
+                    }
+                    if (skip || l > r) {
+                        a.answers[j] = ~0ull;
+                    } else if (p >= k) {
+                        a.answers[j] = (u64)l;
+                    } else {
+                        enq = true;
+                    }
+                    if (a.skipped) {
+                        const u32 sk = __ballot_sync(__activemask(), skip);
+                        if (sk && lane == __ffs(__activemask()) - 1) atomicAdd(a.skipped, (unsigned long long)__popc(sk));
+                    }
+                }
+                const u32 em = __ballot_sync(kFull, enq);
+                if (enq) {
+                    QEntry &e = q[(tail + __popc(em & lt)) & (kQueue - 1)];
+                    e.kmer = km;
+                    e.j = j;
+                    e.l = l;
+                    e.r = r;
+                }
+                tail += __popc(em);
+                if (read_mode) row = __shfl_sync(kFull, rr, cnt - 1);
+                c_next += cnt;
+                __syncwarp();
+            }
+        }
+        // ---- idle lanes pop
+        const bool need = I == kDone;
+        const u32 m = __ballot_sync(kFull, need);
+        const u32 avail = tail - head;
+        if (m == kFull && avail == 0 && !more) break;
+        const u32 take = min((u32)__popc(m), avail);
+        const u32 rank = __popc(m & lt);
+        if (need && rank < take) {
+            const QEntry &e = q[(head + rank) & (kQueue - 1)];
+            kmer = e.kmer;
+            J = e.j;
+            L = e.l;
+            Rr = e.r;
+            I = p;
+        }
+        head += take;
+        __syncwarp();
+        // ---- one step for every active lane
+        if (I != kDone) {
+            const u32 c = (u32)((kmer >> (62u - 2u * I)) & 3u);
+            const typename R::Fetch f = rk.fetch(c, L, Rr, 0);
+            const u32 Cc = c == 0 ? C0 : c == 1 ? C1 : c == 2 ? C2 : C3;
+            rk.finish(f, Cc, L, Rr, 0, kFull);
+            I++;
+            if (L > Rr || I >= k) {
+                a.answers[J] = (L <= Rr) ? (u64)L : ~0ull;
+                I = kDone;
+            }
+        }
+    }
+}
+
 // -------------------------------------------------------------- dispatch
 
 template <class R, int KPT, int TPK>
@@ -191,9 +343,27 @@ int launch_one(const R &rk, SearchArgs &a, const sbwt_index *ix, cudaStream_t s,
     return 0;
 }
 
+template <class R>
+int launch_queue(const R &rk, SearchArgs &a, const sbwt_index *ix, cudaStream_t s, u32 *blocks_out) {
+    auto kern = search_queue_kernel<R>;
+    int per_sm = 0;
+    SBWT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, 0));
+    if (per_sm < 1) per_sm = 1;
+    const u32 blocks = (u32)per_sm * (u32)ix->num_sms;
+    if (blocks_out) *blocks_out = blocks;
+    SBWT_CHECK_CUDA(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), s));
+    kern<<<blocks, 128, 0, s>>>(rk, a);
+    SBWT_CHECK_CUDA(cudaGetLastError());
+    return 0;
+}
+
 template <int TPK>
 int lines_kpt(const sbwt_index *ix, SearchArgs &a, cudaStream_t s, u32 kpt, u32 tpb, u32 *blocks) {
     LinesRankerT<TPK> rk{ix->d_lines, ix->lpc};
+    if constexpr (TPK == 1) {
+        if (kpt == 0) return launch_queue(rk, a, ix, s, blocks);  // kpt 0: the queue-fed form
+    }
+    if (kpt == 0) kpt = 1;
     switch (kpt) {
     case 1: return launch_one<LinesRankerT<TPK>, 1, TPK>(rk, a, ix, s, tpb, blocks);
     case 2: return launch_one<LinesRankerT<TPK>, 2, TPK>(rk, a, ix, s, tpb, blocks);
@@ -209,6 +379,9 @@ template <int SB, int KIND, class IT, int TPK>
 int poppy_kpt(const sbwt_index *ix, SearchArgs &a, cudaStream_t s, u32 kpt, u32 tpb, u32 *blocks) {
     PoppyRanker<SB, KIND, IT, TPK> rk{ix->d_bits, ix->d_L0, ix->d_L12, ix->wpv, ix->l0w, ix->l12w};
     using R = PoppyRanker<SB, KIND, IT, TPK>;
+    if constexpr (sizeof(IT) == 4 && TPK == 1) {
+        if (kpt == 0) return launch_queue(rk, a, ix, s, blocks);
+    }
     if (kpt >= 2 && sizeof(IT) == 4) return launch_one<R, 2, TPK>(rk, a, ix, s, tpb, blocks);
     return launch_one<R, 1, TPK>(rk, a, ix, s, tpb, blocks);
 }
@@ -228,6 +401,7 @@ int poppy_sb(const sbwt_index *ix, SearchArgs &a, cudaStream_t s, const KernelSh
 
 u32 search_chunk(const KernelShape &sh) {
     const u32 groups = 32u / (sh.layout == SBWT_LAYOUT_LINES ? sh.tpk : 1u);
+    if (sh.kpt == 0) return 32u * 16u;  // queue-fed form: 16 fills of 32 per chunk
     return groups * std::max(sh.kpt, 1u) * 8u;
 }
 
