@@ -169,6 +169,21 @@ int sbwt_pack(const uint8_t *d_letters, uint64_t n_letters, uint64_t *d_words, v
 int sbwt_search_reads(sbwt_index *index, const uint8_t *d_letters, uint64_t n_letters, const uint64_t *d_row_starts,
                       uint64_t n_rows, uint64_t *d_answers, uint32_t *d_member_bits, uint64_t n_kmers, void *stream);
 
+/* sbwt_search_reads for callers that cannot allocate device memory at search
+ * time: one capturing the search into its own CUDA graph (cudaMalloc cannot be
+ * captured), or one whose device memory another allocator already holds.  No
+ * counterpart in the reference.  Same arguments and answers as
+ * sbwt_search_reads, but all scratch (packed letters, per-row k-mer table,
+ * chunk table, scan sums, work counter) lives in one fixed 32 MiB device array
+ * of the library (held by every GPU that loads it until exit), so no
+ * cudaMalloc/cudaFree is made; a batch needing more (roughly more than 64M
+ * letters) is rejected with an error.  The first call on a device looks the
+ * array up (cudaGetSymbolAddress): make it before any stream capture.  Calls
+ * share the array: calls that overlap on the GPU race. */
+int sbwt_search_reads_noalloc(sbwt_index *index, const uint8_t *d_letters, uint64_t n_letters,
+                              const uint64_t *d_row_starts, uint64_t n_rows, uint64_t *d_answers,
+                              uint32_t *d_member_bits, uint64_t n_kmers, void *stream);
+
 /* Host-memory form of sbwt_search_reads: letters, row starts and answers
  * are host buffers (pinned or pageable).  The batch is streamed through the
  * GPU in chunks with copies overlapped with compute.  Replaces the

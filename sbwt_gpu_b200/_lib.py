@@ -121,6 +121,8 @@ SIGNATURES = {
     "sbwt_pack": (c_int, [c_void_p, c_uint64, c_void_p, c_void_p]),
     "sbwt_search_reads": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_void_p, c_void_p, c_uint64,
                                   c_void_p]),
+    "sbwt_search_reads_noalloc": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_void_p, c_void_p,
+                                          c_uint64, c_void_p]),
     "sbwt_search_reads_host": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_void_p, c_uint64]),
     "sbwt_count_kmers": (c_uint64, [c_void_p, c_uint64, c_uint32]),
     "sbwt_profile_enable": (c_int, [c_void_p, c_int]),
