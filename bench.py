@@ -57,7 +57,71 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-prefilter", action="store_true", help="skip the learned-prefilter leg")
+    ap.add_argument("--no-autotune", action="store_true", help="skip the autotuned leg")
+    ap.add_argument("--pf-queries", type=int, default=200_000_000)
+    ap.add_argument("--pf-steps", type=int, default=20000)
+    ap.add_argument("--workload", choices=["large", "batched", "pangenome"], default="large",
+                    help="large (default, the headline); batched = 64 files of uneven reads over the small "
+                         "index; pangenome = 20 haplotypes of a 50 Mbp base")
     return ap.parse_args()
+
+
+WORKLOADS = {
+    "large": "large: 100 Mbp genome (41% GC) + 5% repeats, SBWT k=31, p=12, "
+             "10M reads x 150 bp (10% genome-sampled with 1% subs, 90% random)",
+    "batched": "batched: index of the small workload (1 Mbp, k=31); 64 query files, read lengths 70% 150 bp / "
+               "20% lognormal(2 kbp, 1.0) / 10% lognormal(15 kbp, 0.8) in [31, 1e5]; 500M k-mers, 30% of reads "
+               "genome-sampled with 2% subs; one persistent launch",
+    "pangenome": "pangenome: 20 haplotypes of a 50 Mbp base (41% GC), 0.5% SNPs, 0.05% indels of 1-20 bp; SBWT "
+                 "of the union k-mer set, k=31, p=14; 2G k-mers from 150 bp and lognormal 10 kbp reads, "
+                 "95% negatives",
+}
+
+
+def workload_of(args, rank):
+    """(sequences to index, letters, row starts, p) of the selected workload; every rank gets its own reads."""
+    from sbwt_gpu_b200 import workloads as wl
+    if args.workload == "large":
+        genome, letters, rows = workload(args.scale, rank)
+        return [genome], letters, rows, args.p
+    if args.workload == "batched":
+        import sbwt_gpu_b200 as sg
+        genome = wl.config1(seed=1235)["genome"]
+        d = tempfile.mkdtemp(prefix="sbwt_batched_")
+        paths = []
+        total = int(500_000_000 * args.scale)
+        for f, (lt, rw) in enumerate(wl.config3_files(genome, seed=1237 + 100 * rank, total_kmers=total)):
+            path = os.path.join(d, f"q{f:02d}.fa")
+            wl.write_fasta(path, lt, rw)
+            paths.append(path)
+        letters, rows, _, _ = sg.read_queries_many(paths, 31)
+        return [genome], letters, rows, 10
+    # pangenome
+    rng = wl.rng_for(1239)
+    base = wl.random_bases(rng, int(50_000_000 * args.scale), gc=0.41)
+    haps = wl.haplotypes(rng, base, 20)
+    rrng = wl.rng_for(8000 + rank)
+    total = int(2_000_000_000 * args.scale)
+    parts, lens, got = [], [], 0
+    while got < total:
+        long_read = rrng.random() < 0.1
+        ln = int(min(100_000, max(31, rrng.lognormal(np.log(10_000), 0.5)))) if long_read else 150
+        lens.append(ln)
+        got += ln - 30
+    lens = np.array(lens, dtype=np.int64)
+    lens[-1] -= got - total
+    rows = np.zeros(lens.size + 1, dtype=np.uint64)
+    rows[1:] = np.cumsum(lens)
+    letters = wl.ACGT[rrng.integers(0, 4, size=int(rows[-1]), dtype=np.uint8)]
+    pos_rows = np.flatnonzero(rrng.random(lens.size) < 0.05)
+    for r in pos_rows.tolist():  # 5% of reads copied from a haplotype
+        h = haps[r % 20]
+        a, b = int(rows[r]), int(rows[r + 1])
+        if b - a <= h.size:
+            s0 = int(rrng.integers(0, h.size - (b - a) + 1))
+            letters[a:b] = h[s0:s0 + (b - a)]
+    return haps, letters, rows, 14
 
 
 def workload(scale, rank):
@@ -139,10 +203,11 @@ def cpu_reference(ox, letters, rows, k, p, budget_s, table):
     # calibrate on a small prefix, then size the sample to the budget
     r0 = min(rows.size - 1, 2000)
     t = time.perf_counter()
-    ox.search_reads(letters[: int(rows[r0])], rows[: r0 + 1], k, p, table)
-    rate = (r0 * 120) / max(time.perf_counter() - t, 1e-6)
+    a0 = ox.search_reads(letters[: int(rows[r0])], rows[: r0 + 1], k, p, table)
+    rate = a0.size / max(time.perf_counter() - t, 1e-6)
+    per_row = max(a0.size / max(r0, 1), 1.0)
     want_kmers = rate * budget_s
-    nr = int(min(rows.size - 1, max(r0, want_kmers / 120)))
+    nr = int(min(rows.size - 1, max(r0, want_kmers / per_row)))
     sub_rows = rows[: nr + 1]
     sub_letters = letters[: int(sub_rows[-1])]
     t = time.perf_counter()
@@ -175,7 +240,7 @@ def main():
     import sbwt_gpu_b200 as sg
     import oracle as orc
 
-    genome, letters, rows = workload(args.scale, rank)
+    seqs, letters, rows, p = workload_of(args, rank)
     n_kmers = sg.count_kmers(rows, k)
     # the index: rank 0 builds the SBWT and writes the reference's files; every rank loads them
     tmpdir = os.environ.get("SBWT_BENCH_DIR") or os.path.join(tempfile.gettempdir(), f"sbwt_bench_{os.getppid()}")
@@ -183,7 +248,7 @@ def main():
     prefix = os.path.join(tmpdir, "ix")
     if rank == 0:
         t = time.perf_counter()
-        built = sg.build_sbwt([genome.tobytes()], k)
+        built = sg.build_sbwt([x.tobytes() for x in seqs], k)
         build_s = time.perf_counter() - t
         paths = sg.write_index_files(prefix, built)
         n_columns = built.n_bits
@@ -275,6 +340,39 @@ def main():
         e2e = {"value": n_kmers * world * args.e2e_steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(letters.nbytes + rows.nbytes), "d2h_bytes_per_step": int(n_kmers * 8)}
 
+    # ---- autotuned leg: the tuner picks shape and presearch depth on a sample, then the batch is timed again
+    tuned = None
+    if not args.no_autotune and rank == 0:
+        ns = min(rows.size - 1, 1_000_000)
+        nk_s = sg.count_kmers(rows[: ns + 1], k)
+        d_ls = torch.from_numpy(letters[: int(rows[ns])]).to(dev)
+        d_rs = torch.from_numpy(rows[: ns + 1].view(np.int64)).to(dev)
+        rep = ix.autotune(d_ls, d_rs, d_ans, nk_s, tune_p=True, tune_poppy=True)
+        del d_ls, d_rs
+        ix.profile(True)
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize(dev)
+        ev0.record(stream)
+        t_ms = []
+        for _ in range(args.steps):
+            step()
+            t_ms.append(ix.last_profile()["search_ms"])
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        tt = ev0.elapsed_time(ev1)
+        got = d_ans[: ans.size].cpu().numpy().view(np.uint64)
+        if not np.array_equal(got, ans):
+            raise SystemExit("bench: autotuned answers differ from the oracle")
+        tuned = {"value": n_kmers * args.steps / (tt / 1e3), "ms_per_step": tt / args.steps,
+                 "search_kernel_ms": statistics.mean(t_ms), "choice": rep["best"],
+                 "candidates": len(rep["candidates"]), "tuned_on_kmers": nk_s}
+
+    # ---- learned-prefilter leg (the prefilter configuration: index of the small workload, 90% negatives)
+    prefilter = None
+    if not args.no_prefilter and rank == 0:
+        prefilter = prefilter_leg(args, dev, k)
+
     if rank == 0:
         peak, peak_kind = measured_hbm()
         kern_ms = statistics.mean(search_ms)
@@ -294,9 +392,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded)",
             "config": {
-                "workload": "large: 100 Mbp genome (41% GC) + 5% repeats, SBWT k=31, p=12, "
-                            "10M reads x 150 bp (10% genome-sampled with 1% subs, 90% random)"
-                if args.scale == 1.0 else f"large x{args.scale}",
+                "workload": WORKLOADS[args.workload] if args.scale == 1.0 else f"{args.workload} x{args.scale}",
                 "n_kmers_per_gpu": n_kmers, "n_columns": info["n_bits"], "k": k, "p": p,
                 "layout": args.layout, "present_kmers": hits,
                 "l2": "inputs and outputs larger than L2 (letters %.2f GB, answers %.2f GB); no flush" % (
@@ -312,6 +408,8 @@ def main():
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,
+            "autotuned": tuned,
+            "prefilter": prefilter,
         }
         print(json.dumps(line), flush=True)
     ix.close()
@@ -321,11 +419,69 @@ def main():
     return 0
 
 
+def prefilter_leg(args, dev, k):
+    """Plain vs learned-prefiltered search of 200M single k-mers (90% negatives: half uniform random, half
+    indexed k-mers with 1-3 substitutions) against the index of the small workload (1 Mbp uniform genome,
+    p = 10); the MLP is trained on the GPU (20k Adam steps, batch 8192, 5e7 + 5e7 candidates)."""
+    import torch
+    import sbwt_gpu_b200 as sg
+    from sbwt_gpu_b200 import workloads as wl
+    w = wl.config1(seed=1235)
+    built = sg.build_sbwt([w["genome"].tobytes()], k)
+    pix = sg.Index.from_bits(built.bits, built.n_bits, k=k, k_presearch=10)
+    t = time.perf_counter()
+    pf = sg.Prefilter.train(pix, steps=args.pf_steps, batch=8192, n_positive=50_000_000, n_negative=50_000_000,
+                            seed=4)
+    train_s = time.perf_counter() - t
+    st = pf.stats()
+    kmers = wl.kmer_query_words(wl.rng_for(4242), w["genome"], args.pf_queries, k, neg_frac=0.9)
+    d_k = torch.from_numpy(kmers.view(np.int64)).to(dev)
+    del kmers
+    plain = torch.empty_like(d_k)
+    filt = torch.empty_like(d_k)
+    d_l = torch.empty(d_k.numel(), dtype=torch.float32, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps
+
+    n = d_k.numel()
+    reps = max(args.steps, 3)
+    ms_plain = timed(lambda: pix.search_kmers(d_k, plain), reps)
+    ms_logits = timed(lambda: pf.logits(d_k, d_l), reps)
+    ms_filt = timed(lambda: pix.search_kmers_filtered(pf, d_k, filt), reps)
+    skipped = pix.search_kmers_filtered(pf, d_k, filt)
+    torch.cuda.synchronize(dev)
+    p_np, f_np = plain.cpu().numpy().view(np.uint64), filt.cpu().numpy().view(np.uint64)
+    nf = 0xFFFFFFFFFFFFFFFF
+    false_absent = int(((p_np != nf) & (f_np == nf)).sum())
+    res = {
+        "workload": "prefilter: index of the small workload (1 Mbp uniform genome, k=31, p=10); "
+                    f"{n} single k-mers, 90% negatives (half uniform random, half 1-3 substitutions)",
+        "plain_kmers_per_s": n / (ms_plain / 1e3), "prefiltered_kmers_per_s": n / (ms_filt / 1e3),
+        "speedup": ms_plain / ms_filt, "mlp_kmers_per_s": n / (ms_logits / 1e3),
+        "mlp_tflops": n * 2 * (128 * 256 + 256 * 256 + 256) / (ms_logits / 1e3) / 1e12,
+        "skip_rate": skipped / n, "false_absent": false_absent, "bit_exact": bool(np.array_equal(p_np, f_np)),
+        "present": int((p_np != nf).sum()), "train_s": round(train_s, 2), "train": st,
+    }
+    pf.close()
+    pix.close()
+    return res
+
+
 def reference_arm(args, k, p):
     import oracle as orc
     import sbwt_gpu_b200 as sg
-    genome, letters, rows = workload(args.scale, 0)
-    built = sg.build_sbwt([genome.tobytes()], k)
+    seqs, letters, rows, p = workload_of(args, 0)
+    built = sg.build_sbwt([x.tobytes() for x in seqs], k)
     ox = orc.OracleIndex(built.bits, built.n_bits)
     del built
     table = ox.presearch(p) if p else None
@@ -347,8 +503,8 @@ def reference_arm(args, k, p):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded)",
-        "config": {"workload": "large: 100 Mbp genome (41% GC) + 5% repeats, SBWT k=31, p=12, "
-                               "10M reads x 150 bp (10% genome-sampled with 1% subs, 90% random)", "k": k, "p": p},
+        "config": {"workload": WORKLOADS[args.workload] if args.scale == 1.0 else f"{args.workload} x{args.scale}",
+                   "k": k, "p": p},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

@@ -203,3 +203,51 @@ def write_fasta(path, letters, row_starts, width=None):
             f.write(b">r%d\n" % i)
             f.write(letters[rs[i]:rs[i + 1]].tobytes())
             f.write(b"\n")
+
+
+def pack_words(seq):
+    """ASCII ACGT -> MSB-first 2-bit words (letter i of word w at bits 63-2i..62-2i), plus one zero word."""
+    codes = np.searchsorted(ACGT, seq).astype(np.uint64)
+    n = codes.size
+    nw = (n + 31) // 32 + 1
+    padded = np.zeros(nw * 32, dtype=np.uint64)
+    padded[:n] = codes
+    p = padded.reshape(nw, 32)
+    words = np.zeros(nw, dtype=np.uint64)
+    for i in range(32):
+        words |= p[:, i] << np.uint64(62 - 2 * i)
+    return words
+
+
+def kmer_query_words(rng, genome, n, k, neg_frac=0.9, chunk=10_000_000):
+    """n k-mers as MSB-first u64 words: (1-neg_frac) sampled from the genome, neg_frac/2 uniform random,
+    neg_frac/2 genome k-mers with 1-3 substitutions; shuffled."""
+    words = pack_words(genome)
+    mask = np.uint64(((1 << (2 * k)) - 1) << (64 - 2 * k)) if k < 32 else np.uint64(0xFFFFFFFFFFFFFFFF)
+    out = np.empty(n, dtype=np.uint64)
+    n_neg = int(n * neg_frac)
+    kinds = np.zeros(n, dtype=np.uint8)  # 0 genome, 1 random, 2 mutated
+    kinds[: n_neg // 2] = 1
+    kinds[n_neg // 2: n_neg] = 2
+    rng.shuffle(kinds)
+    for a in range(0, n, chunk):
+        b = min(n, a + chunk)
+        kd = kinds[a:b]
+        pos = rng.integers(0, genome.size - k + 1, size=b - a).astype(np.uint64)
+        wi = (pos >> np.uint64(5)).astype(np.int64)
+        sh = (pos & np.uint64(31)) * np.uint64(2)
+        hi = words[wi] << sh
+        lo = np.where(sh == 0, np.uint64(0), words[wi + 1] >> (np.uint64(64) - np.where(sh == 0, np.uint64(1), sh)))
+        x = (hi | lo) & mask
+        mut = kd == 2
+        nsub = rng.integers(1, 4, size=b - a)
+        for s in range(3):
+            sel = mut & (nsub > s)
+            p = rng.integers(0, k, size=b - a).astype(np.uint64)
+            shift = np.uint64(62) - np.uint64(2) * p
+            old = (x >> shift) & np.uint64(3)
+            new = (old + rng.integers(1, 4, size=b - a).astype(np.uint64)) & np.uint64(3)
+            x = np.where(sel, (x & ~(np.uint64(3) << shift)) | (new << shift), x)
+        rnd = rng.integers(0, 2**63, size=b - a, dtype=np.int64).astype(np.uint64) * np.uint64(2) & mask
+        out[a:b] = np.where(kd == 1, rnd, x)
+    return out
