@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-prefilter", action="store_true", help="skip the learned-prefilter leg")
     ap.add_argument("--no-autotune", action="store_true", help="skip the autotuned leg")
+    ap.add_argument("--no-per-kmer", action="store_true", help="skip the leg that searches every k-mer")
+    ap.add_argument("--search-every-kmer", action="store_true",
+                    help="main leg without the absent-run skip (every k-mer searched, as the reference does)")
     ap.add_argument("--pf-queries", type=int, default=200_000_000)
     ap.add_argument("--pf-steps", type=int, default=20000)
     ap.add_argument("--workload", choices=["large", "batched", "pangenome"], default="large",
@@ -216,6 +219,42 @@ def cpu_reference(ox, letters, rows, k, p, budget_s, table):
     return ans.size / dt, ans, steps, nr, threads
 
 
+def searched_fraction(ans, steps, rows, k, p, max_rows=20000):
+    """Share of k-mers the run walk actually searches (right to left per read; a search that fails
+    after m letters settles k-m+1 k-mers), from per-k-mer oracle answers and step counts."""
+    import oracle as orc
+    searched = total = 0
+    j0 = 0
+    for r in range(min(rows.size - 1, max_rows)):
+        n = int(rows[r + 1] - rows[r]) - k + 1
+        if n <= 0:
+            continue
+        if j0 + n > ans.size:
+            break
+        j = j0 + n - 1
+        while j >= j0:
+            searched += 1
+            if ans[j] != orc.NOT_FOUND:
+                j -= 1
+            else:
+                j -= k - min(max(p, p + int(steps[j])), k) + 1
+        j0 += n
+        total += n
+    return searched / max(total, 1)
+
+
+def kernel_traffic(kernel, workload, n_kmers):
+    """DRAM bytes of one launch from the committed ncu summary, if it covers this kernel and workload."""
+    tp = os.path.join(ROOT, "profiles", "search_kernel_traffic.json")
+    try:
+        for e in json.load(open(tp))["entries"]:
+            if e["kernel"] == kernel and e["workload"] == workload:
+                return float(e["dram_bytes_per_kmer"]) * n_kmers, e
+    except (OSError, ValueError, KeyError, TypeError):
+        pass
+    return None, None
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -259,7 +298,10 @@ def main():
     layout = sg.SBWT_LAYOUT_POPPY if args.layout == "poppy" else sg.SBWT_LAYOUT_LINES
     t = time.perf_counter()
     ix = sg.Index.load(*paths, k=k, k_presearch=p, device=local_rank, layout=layout,
-                       kmers_per_thread=args.kpt, threads_per_kmer=args.tpk, threads_per_block=args.tpb)
+                       kmers_per_thread=args.kpt, threads_per_kmer=args.tpk, threads_per_block=args.tpb,
+                       skip_absent_runs=0 if args.search_every_kmer else 1)
+    runs_form = args.kpt == 0 and not args.search_every_kmer and (args.tpk <= 1 or args.layout == "poppy")
+    kernel = "search_runs_kernel" if runs_form else ("search_queue_kernel" if args.kpt == 0 else "search_kernel")
     load_s = time.perf_counter() - t
     info = ix.info()
 
@@ -312,6 +354,7 @@ def main():
         if not np.array_equal(got, ans):
             raise SystemExit(f"bench: {int((got != ans).sum())} of {ans.size} sampled answers differ from the oracle")
         mean_steps = float(steps.mean())
+        searched = searched_fraction(ans, steps, rows, k, p) if runs_form else 1.0
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"first {nr} reads ({ans.size} k-mers) of the same batch, C restatement of the reference "
                          f"search (the reference has no CPU search), OpenMP schedule(dynamic,4096)"}
@@ -339,6 +382,29 @@ def main():
             raise SystemExit("bench: end-to-end answers differ from the oracle")
         e2e = {"value": n_kmers * world * args.e2e_steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(letters.nbytes + rows.nbytes), "d2h_bytes_per_step": int(n_kmers * 8)}
+
+    # ---- the same batch with every k-mer searched (the reference's per-k-mer work), for comparison
+    per_kmer = None
+    if runs_form and not args.no_per_kmer and rank == 0:
+        ix.profile(True)
+        ix.set_absent_skip(False)
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize(dev)
+        ev0.record(stream)
+        t_ms = []
+        for _ in range(args.steps):
+            step()
+            t_ms.append(ix.last_profile()["search_ms"])
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        tt = ev0.elapsed_time(ev1)
+        ix.set_absent_skip(True)
+        got = d_ans[: ans.size].cpu().numpy().view(np.uint64)
+        if not np.array_equal(got, ans):
+            raise SystemExit("bench: per-k-mer answers differ from the oracle")
+        per_kmer = {"value": n_kmers * args.steps / (tt / 1e3), "ms_per_step": tt / args.steps,
+                    "search_kernel_ms": statistics.mean(t_ms), "kernel": "search_queue_kernel"}
 
     # ---- autotuned leg: the tuner picks shape and presearch depth on a sample, then the batch is timed again
     tuned = None
@@ -379,13 +445,7 @@ def main():
         q = (letters.size / 4.0) / n_kmers
         b_kmer = 128.0 * mean_steps + 16 + 8 + q
         achieved = n_kmers * b_kmer / (kern_ms / 1e3) / 1e9
-        traffic = None
-        tp = os.path.join(ROOT, "profiles", "search_kernel_traffic.json")
-        if os.path.exists(tp):
-            try:
-                traffic = float(json.load(open(tp))["dram_bytes_per_kmer"]) * n_kmers
-            except Exception:
-                traffic = None
+        traffic, tr = kernel_traffic(kernel, args.workload if args.scale == 1.0 else None, n_kmers)
         hits = int((d_ans.cpu().numpy().view(np.uint64) != orc.NOT_FOUND).sum())
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -402,12 +462,15 @@ def main():
             },
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": f"of {peak_kind}",
-                         "kernel": "search_kernel", "kernel_ms": kern_ms, "bytes_per_kmer_model": b_kmer,
-                         "mean_steps": mean_steps},
+                         "kernel": kernel, "kernel_ms": kern_ms, "bytes_per_kmer_model": b_kmer,
+                         "mean_steps": mean_steps, "searched_fraction": searched,
+                         "dram_frac": (traffic / (kern_ms / 1e3) / 1e9 / peak) if traffic else None,
+                         "traffic_source": tr["source"] if tr else None},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,
+            "per_kmer": per_kmer,
             "autotuned": tuned,
             "prefilter": prefilter,
         }

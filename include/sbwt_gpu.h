@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define SBWT_GPU_ABI_VERSION 1
+#define SBWT_GPU_ABI_VERSION 2
 
 /* Rank-structure kinds of the reference (include/enums.hpp:9-11). */
 #define SBWT_POPPY 1
@@ -56,6 +56,11 @@ typedef struct {
     uint32_t kmers_per_thread;   /* search kernel: 0 = one k-mer per lane fed from a per-warp queue
                                     (default); 1,2,3,4,6,8 = k-mer slots held in registers */
     uint32_t threads_per_kmer;   /* search kernel: lanes sharing one k-mer, 1|2|4 (0 = default) */
+    int32_t skip_absent_runs;    /* searches of reads with the queue-fed kernel: 1 (default) = walk each
+                                    read from right to left and, when a k-mer's search fails after m
+                                    letters, answer the k-m+1 k-mers that contain those m letters as
+                                    absent without searching them; 0 = search every k-mer.  The
+                                    answers are the same either way.  No reference counterpart. */
 } sbwt_params;
 
 /* Fills the defaults (k=30, p=12, SB=1024, poppy, no shuffles, device 0,
@@ -119,6 +124,11 @@ int sbwt_rank_export(sbwt_index *index, uint32_t bits_in_superblock, int32_t ran
 int sbwt_configure(sbwt_index *index, int32_t layout, uint32_t bits_in_superblock, int32_t rank_structure,
                    int32_t with_shuffles, uint32_t kmers_per_thread, uint32_t threads_per_kmer,
                    uint32_t threads_per_block);
+
+/* Turns the absent-run skip of sbwt_params.skip_absent_runs on (1) or off
+ * (0) for later searches of reads on this index.  No reference counterpart:
+ * the reference searches every k-mer (include/gpu/search_kernel.hpp:61-104). */
+int sbwt_set_absent_skip(sbwt_index *index, int32_t on);
 
 /* Sets the L2 fetch granularity (32, 64 or 128 bytes; cudaLimitMaxL2FetchGranularity)
  * of the index's device for this process, as the reference does before its

@@ -143,6 +143,10 @@ class Index:
         check(lib.sbwt_configure(self._h, layout, bits_in_superblock, rank_structure, int(with_shuffles),
                                  kmers_per_thread, threads_per_kmer, threads_per_block))
 
+    def set_absent_skip(self, on):
+        """Absent-run skip for searches of reads (on by default; answers are the same either way)."""
+        check(lib.sbwt_set_absent_skip(self._h, 1 if on else 0))
+
     def autotune(self, d_letters, d_row_starts, d_answers, n_kmers, tune_p=False, tune_poppy=False):
         """Times candidate launch shapes on a device sample, keeps the fastest; returns the JSON report."""
         n_rows = int(d_row_starts.numel()) - 1

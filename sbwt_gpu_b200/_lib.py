@@ -32,6 +32,7 @@ class Params(ctypes.Structure):
         ("layout", c_int32),
         ("kmers_per_thread", c_uint32),
         ("threads_per_kmer", c_uint32),
+        ("skip_absent_runs", c_int32),
     ]
 
 
@@ -117,6 +118,7 @@ SIGNATURES = {
     "sbwt_presearch_export": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64]),
     "sbwt_rank_export": (c_int, [c_void_p, c_uint32, c_int32, c_int, c_void_p, c_uint64, c_void_p, c_uint64]),
     "sbwt_configure": (c_int, [c_void_p, c_int32, c_uint32, c_int32, c_int32, c_uint32, c_uint32, c_uint32]),
+    "sbwt_set_absent_skip": (c_int, [c_void_p, c_int32]),
     "sbwt_search_packed": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_void_p]),
     "sbwt_pack": (c_int, [c_void_p, c_uint64, c_void_p, c_void_p]),
     "sbwt_search_reads": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_void_p, c_void_p, c_uint64,

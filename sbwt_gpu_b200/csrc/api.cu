@@ -88,6 +88,7 @@ void apply_shape(sbwt_index *ix, const sbwt_params *p) {
     sh.sb = p->bits_in_superblock;
     sh.kind = p->rank_structure;
     sh.shuffles = p->with_shuffles;
+    sh.skip = p->skip_absent_runs ? 1 : 0;
 }
 
 // Shared tail of the two index constructors: `words[c]` hold ceil(n/64)
@@ -222,6 +223,7 @@ extern "C" int sbwt_params_default(sbwt_params *p) {
     p->layout = SBWT_LAYOUT_LINES;
     p->kmers_per_thread = 0;
     p->threads_per_kmer = 0;
+    p->skip_absent_runs = 1;
     return 0;
 }
 
@@ -355,10 +357,17 @@ extern "C" int sbwt_configure(sbwt_index *ix, int32_t layout, uint32_t sb, int32
     return 0;
 }
 
+extern "C" int sbwt_set_absent_skip(sbwt_index *ix, int32_t on) {
+    clear_error();
+    if (!ix) return set_error("index is NULL");
+    ix->shape.skip = on ? 1 : 0;
+    return 0;
+}
+
 namespace sbwt {
 namespace {
 
-SearchArgs base_args(const sbwt_index *ix) {
+SearchArgs base_args(const sbwt_index *ix, bool rows) {
     SearchArgs a;
     std::memset(&a, 0, sizeof(a));
     a.lines = ix->d_lines;
@@ -373,7 +382,8 @@ SearchArgs base_args(const sbwt_index *ix) {
     a.pre = ix->d_pre;
     a.p = ix->p;
     a.k = ix->k;
-    a.chunk = search_chunk(ix->shape);
+    a.chunk = search_chunk(ix, rows);
+    a.runs = rows && runs_form(ix);
     return a;
 }
 
@@ -387,7 +397,7 @@ int search_rows_device(sbwt_index *ix, Workspace &w, const uint8_t *d_letters, u
                        u64 n_rows, u64 *d_answers, uint32_t *d_member, u64 n_kmers, cudaStream_t s) {
     if (n_rows == 0 || n_kmers == 0) return 0;
     const u64 n_words = (n_letters + 32 + 31) / 32;
-    SearchArgs a = base_args(ix);
+    SearchArgs a = base_args(ix, true);
     SBWT_TRY(grow(w.words, w.words_cap, n_words));
     SBWT_TRY(grow(w.kstart, w.kstart_cap, n_rows + 1));
     SBWT_TRY(grow(w.scan, w.scan_cap, scan_scratch_words(n_rows)));
@@ -402,7 +412,8 @@ int search_rows_device(sbwt_index *ix, Workspace &w, const uint8_t *d_letters, u
         const KernelShape &sh = ix->shape;
         const uint64_t key[12] = {(uint64_t)d_letters, n_letters, (uint64_t)d_rows, n_rows, (uint64_t)d_answers,
                                   (uint64_t)d_member, n_kmers, (uint64_t)s, ix->gen,
-                                  ((uint64_t)sh.layout << 48) | ((uint64_t)sh.kpt << 32) | ((uint64_t)sh.tpk << 16) | sh.tpb,
+                                  ((uint64_t)sh.layout << 48) | ((uint64_t)sh.skip << 40) | ((uint64_t)sh.kpt << 32) |
+                                      ((uint64_t)sh.tpk << 16) | sh.tpb,
                                   (uint64_t)w.words ^ (uint64_t)w.kstart, (uint64_t)w.chunk_row ^ (uint64_t)w.counter};
         if (w.graph && std::memcmp(key, w.graph_key, sizeof key) == 0) {
             SBWT_CHECK_CUDA(cudaGraphLaunch(w.graph, s));
@@ -480,7 +491,7 @@ extern "C" int sbwt_search_packed(sbwt_index *ix, const uint64_t *d_kmer_string,
     cudaStream_t s = (cudaStream_t)stream;
     Workspace &w = ix->ws[0];
     SBWT_TRY(grow(w.counter, w.counter_cap, 1));
-    SearchArgs a = base_args(ix);
+    SearchArgs a = base_args(ix, false);
     a.words = d_kmer_string;
     a.positions = d_positions_in_results_out;
     a.max_pos = (n_words - 1) * 32 - 1;

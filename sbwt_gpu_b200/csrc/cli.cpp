@@ -83,6 +83,7 @@ int parse(int argc, char **argv, Options &o) {
             std::fprintf(stderr, "Ignoring %s.\n", s.c_str());
         } else if (s == "--layout=lines") o.p.layout = SBWT_LAYOUT_LINES;
         else if (s == "--layout=poppy") o.p.layout = SBWT_LAYOUT_POPPY;
+        else if (s == "--search-every-kmer") o.p.skip_absent_runs = 0;
         else if (std::regex_match(s, m, sb_re)) o.p.bits_in_superblock = (uint32_t)std::stoul(m[1]);
         else if (std::regex_match(s, m, lp_re)) o.limit_presearch = std::stoi(m[1]);
         else if (std::regex_match(s, m, ls_re)) o.limit_search = std::stoi(m[1]);

@@ -37,7 +37,8 @@ struct SearchArgs {
     u64 *answers;
     u64 n_kmers;
     unsigned long long *counter;  // work-stealing cursor (zeroed before launch)
-    u32 chunk;                    // k-mers per grab
+    u32 chunk;                    // k-mers per grab; with `runs`, k-mers per window of chunk_row
+    u32 runs;                     // read mode: walk runs right to left with the absent-run skip
     // k-mer list mode: k-mer j is kmer_list[j] (MSB-first word)
     const u64 *kmer_list;
     // learned prefilter: skip k-mer j if logits[j] < tau and the Bloom filter rejects it
@@ -57,6 +58,7 @@ struct KernelShape {
     u32 sb = 1024;
     int kind = SBWT_POPPY;
     int shuffles = 0;
+    int skip = 1;  // read mode, queue-fed form: absent-run skip (search_runs_kernel)
 };
 
 // Device buffers of one in-flight search (grow-only).
@@ -152,7 +154,12 @@ template <class T> int grow_host(T *&p, size_t &cap, size_t need);
 
 // search.cu
 int launch_search(const sbwt_index *ix, SearchArgs &a, cudaStream_t s, uint32_t *launched_blocks);
-u32 search_chunk(const KernelShape &sh);
+// Whether a batch of reads searched with the index's current shape runs the
+// run-walking kernel with the absent-run skip.
+bool runs_form(const sbwt_index *ix);
+// Work granularity of a launch: k-mers per grab, or for the run-walking form
+// k-mers per window of the row table.  `rows`: a batch of reads.
+u32 search_chunk(const sbwt_index *ix, bool rows);
 bool search_shape_supported(const KernelShape &sh, bool wide);
 
 }  // namespace sbwt

@@ -67,7 +67,7 @@ extern "C" int sbwt_search_reads_noalloc(sbwt_index *ix, const uint8_t *d_letter
     if (!d_letters || !d_row_starts || !d_answers) return set_error("NULL device pointer");
     SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
     const cudaStream_t s = (cudaStream_t)stream;
-    const u32 chunk = search_chunk(ix->shape);
+    const u32 chunk = search_chunk(ix, true);
     // scratch layout: counter | kstart | scan block sums | chunk table | packed words
     const u64 n_words = (n_letters + 32 + 31) / 32;
     const size_t off_kstart = 256;
@@ -105,6 +105,7 @@ extern "C" int sbwt_search_reads_noalloc(sbwt_index *ix, const uint8_t *d_letter
     a.p = ix->p;
     a.k = ix->k;
     a.chunk = chunk;
+    a.runs = runs_form(ix);
     a.words = words;
     a.row_starts = d_row_starts;
     a.kstart = kstart;

@@ -213,7 +213,7 @@ int search_list(sbwt_index *ix, const uint64_t *d_kmers, uint64_t n, uint64_t *d
     a.pre = ix->d_pre;
     a.p = ix->p;
     a.k = ix->k;
-    a.chunk = search_chunk(ix->shape);
+    a.chunk = search_chunk(ix, false);
     a.kmer_list = d_kmers;
     a.answers = d_answers;
     a.n_kmers = n;

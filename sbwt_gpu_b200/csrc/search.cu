@@ -327,6 +327,159 @@ __global__ void __launch_bounds__(128) search_queue_kernel(const R rk, const Sea
     }
 }
 
+// ------------------------------------------------------- absent-run skip
+//
+// Reads only.  The search of a string s (|s| <= k) ends with a non-empty
+// interval exactly when s is a substring of some indexed k-mer: the interval
+// holds the nodes whose label ends with s, and every substring of an indexed
+// k-mer ends the label of some node (follow predecessor k-mers leftwards;
+// a k-mer without one keeps its $-padded prefixes as dummy nodes).  So when
+// the search of the k-mer starting at j empties after m letters, x[j, j+m)
+// lies in no indexed k-mer, and no k-mer containing it is indexed: the
+// k-mers starting at j+m-k .. j are all absent.  An empty presearch entry
+// gives m = p.  This kernel walks each run of k-mers of one row from right
+// to left and, after a search that fails at m letters, moves left by k-m+1
+// k-mers at once.  Their answers are the ~0 written when the run's window
+// was taken, so every answer equals the reference's per-k-mer search.
+//
+// Work split: a warp takes 32 windows of kWin consecutive k-mer indices from
+// the global cursor and writes ~0 to all their answers (coalesced).  Each
+// lane cuts its window at row ends into runs and enqueues one run per fill
+// into the warp's shared-memory queue; an idle lane pops a run.  Every loop
+// iteration a lane either starts its run's next k-mer (letters + presearch
+// entry, followed by its first step) or takes one rank-pair step.
+
+constexpr u32 kWin = 32;            // k-mers per window (granularity of chunk_row)
+constexpr u32 kStart = 0xfffffffeu; // lane state: start the run's current k-mer
+
+struct RunEntry {
+    u64 pos;  // letter offset of the run's last (rightmost) k-mer
+    u64 j;    // k-mer index of that k-mer
+    u32 len;  // k-mers in the run, 1..kWin
+};
+
+template <class R>
+__global__ void __launch_bounds__(128) search_runs_kernel(const R rk, const SearchArgs a) {
+    static_assert(sizeof(typename R::IT) == 4, "the run form serves 32-bit intervals");
+    __shared__ RunEntry queue[kQueueWarps][kQueue];
+    using PT = uint2;
+    const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const u32 lt = (1u << lane) - 1u;
+    const u32 k = a.k, p = a.p;
+    const u32 C0 = (u32)a.C[0], C1 = (u32)a.C[1], C2 = (u32)a.C[2], C3 = (u32)a.C[3];
+    const u32 rootR = (u32)(a.C[4] - 1ull);
+    const PT *pre = reinterpret_cast<const PT *>(a.pre);
+    const u64 n_eff = min(a.n_kmers, a.kstart[a.n_rows]);
+    RunEntry *q = queue[warp];
+
+    u32 head = 0, tail = 0;  // warp-uniform
+    bool more = true;
+    u64 pj = 0, pe = 0, prow = 0;  // this lane's window: next k-mer to cut, end, row of pj
+    u64 kmer = 0, J = 0, pos = 0;  // current k-mer of this lane's run
+    u32 left = 0;                  // k-mers of the run left of J
+    u32 L = 0, Rr = 0, I = kDone;
+
+    for (;;) {
+        // ---- fill: new windows once every lane's window is cut, then one run per lane
+        if (more && tail - head < 32u) {
+            if (__ballot_sync(kFull, pj < pe) == 0) {
+                unsigned long long base = 0;
+                if (lane == 0) base = atomicAdd(a.counter, (unsigned long long)(32u * kWin));
+                base = __shfl_sync(kFull, base, 0);
+                if (base >= n_eff) {
+                    more = false;
+                } else {
+                    const u64 end = min((u64)base + 32u * kWin, n_eff);
+                    for (u64 t = base + lane; t < end; t += 32u) a.answers[t] = ~0ull;
+                    pj = min((u64)base + (u64)lane * kWin, end);
+                    pe = min(pj + kWin, end);
+                    if (pj < pe) prow = a.chunk_row[pj / kWin];
+                }
+            }
+            if (more) {
+                const bool emit = pj < pe;
+                RunEntry e;
+                if (emit) {
+                    while (a.kstart[prow + 1] <= pj) prow++;  // rows shorter than k hold no k-mers
+                    const u64 last = min(pe, a.kstart[prow + 1]) - 1u;
+                    e.pos = a.row_starts[prow] + (last - a.kstart[prow]);
+                    e.j = last;
+                    e.len = (u32)(last - pj + 1u);
+                    pj = last + 1u;
+                }
+                const u32 em = __ballot_sync(kFull, emit);
+                if (emit) q[(tail + __popc(em & lt)) & (kQueue - 1)] = e;
+                tail += __popc(em);
+                __syncwarp();
+            }
+        }
+        // ---- idle lanes pop a run
+        const bool need = I == kDone;
+        const u32 m = __ballot_sync(kFull, need);
+        const u32 avail = tail - head;
+        if (m == kFull && avail == 0 && !more) break;
+        const u32 take = min((u32)__popc(m), avail);
+        const u32 rank = __popc(m & lt);
+        if (need && rank < take) {
+            const RunEntry &e = q[(head + rank) & (kQueue - 1)];
+            pos = e.pos;
+            J = e.j;
+            left = e.len - 1u;
+            I = kStart;
+        }
+        head += take;
+        __syncwarp();
+        // ---- start: letters (search_kernel.hpp:66-68) and presearch entry (:71-82)
+        u32 adv = 0;  // k-mers settled at and left of J
+        if (I == kStart) {
+            const u64 b = min(pos, a.max_pos) << 1;
+            const u64 w0 = a.words[b >> 6], w1 = a.words[(b >> 6) + 1];
+            const u32 sh = (u32)(b & 63u);
+            kmer = (w0 << sh) | (shr_clamp(w1, 63u - sh) >> 1);
+            if (p) {
+                const PT e = pre[kmer >> (64u - 2u * p)];
+                L = e.x;
+                Rr = e.y;
+            } else {
+                L = 0;
+                Rr = rootR;
+            }
+            if (L > Rr) {
+                adv = k - p + 1u;  // x[J, J+p) is in no indexed k-mer
+            } else if (p >= k) {
+                a.answers[J] = (u64)L;
+                adv = 1;
+            } else {
+                I = p;
+            }
+        }
+        // ---- one rank-pair step (:84-96)
+        if (I < k) {
+            const u32 c = (u32)((kmer >> (62u - 2u * I)) & 3u);
+            const typename R::Fetch f = rk.fetch(c, L, Rr, 0);
+            const u32 Cc = c == 0 ? C0 : c == 1 ? C1 : c == 2 ? C2 : C3;
+            rk.finish(f, Cc, L, Rr, 0, kFull);
+            I++;
+            if (L > Rr) {
+                adv = k - I + 1u;  // x[J, J+I) is in no indexed k-mer
+            } else if (I == k) {
+                a.answers[J] = (u64)L;
+                adv = 1;
+            }
+        }
+        if (adv) {
+            if (adv > left) {
+                I = kDone;
+            } else {
+                left -= adv;
+                J -= adv;
+                pos -= adv;
+                I = kStart;
+            }
+        }
+    }
+}
+
 // -------------------------------------------------------------- dispatch
 
 template <class R, int KPT, int TPK>
@@ -345,7 +498,7 @@ int launch_one(const R &rk, SearchArgs &a, const sbwt_index *ix, cudaStream_t s,
 
 template <class R>
 int launch_queue(const R &rk, SearchArgs &a, const sbwt_index *ix, cudaStream_t s, u32 *blocks_out) {
-    auto kern = search_queue_kernel<R>;
+    auto kern = a.runs ? search_runs_kernel<R> : search_queue_kernel<R>;
     int per_sm = 0;
     SBWT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, 0));
     if (per_sm < 1) per_sm = 1;
@@ -399,7 +552,17 @@ int poppy_sb(const sbwt_index *ix, SearchArgs &a, cudaStream_t s, const KernelSh
 
 }  // namespace
 
-u32 search_chunk(const KernelShape &sh) {
+bool runs_form(const sbwt_index *ix) {
+    const KernelShape &sh = ix->shape;
+    if (!sh.skip || sh.kpt != 0) return false;
+    if (sh.layout == SBWT_LAYOUT_LINES) return ix->lines_ok && sh.tpk == 1;
+    // poppy: the queue-fed forms are the 32-bit single-lane ones
+    return ix->n < (1ull << 32) && !(sh.shuffles && (ix->sb == 1024 || ix->sb == 2048));
+}
+
+u32 search_chunk(const sbwt_index *ix, bool rows) {
+    const KernelShape &sh = ix->shape;
+    if (rows && runs_form(ix)) return kWin;
     const u32 groups = 32u / (sh.layout == SBWT_LAYOUT_LINES ? sh.tpk : 1u);
     if (sh.kpt == 0) return 32u * 16u;  // queue-fed form: 16 fills of 32 per chunk
     return groups * std::max(sh.kpt, 1u) * 8u;

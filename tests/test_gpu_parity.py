@@ -342,3 +342,55 @@ def test_many_files_one_batch(small, cuda, tmp_path):
     with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=10) as ix:
         got = run_reads(ix, letters, rows, cuda)
     assert np.array_equal(got, np.concatenate(wants))
+
+
+def _row_mixture(rng, genome, k):
+    """Rows of every length class the run walk cuts differently: shorter than k, exactly k
+    (one k-mer), a window and a bit, long genome substrings (every k-mer present), random
+    and mutated reads, and many one-k-mer rows in a row."""
+    parts = []
+    for n in [k - 1, k, k + 1, 2 * k, k + 33, k + 64, 1000, 5000]:
+        s = int(rng.integers(0, genome.size - n))
+        parts.append(genome[s:s + n])
+        parts.append(wl.random_bases(rng, n))
+        mut = genome[s:s + n].copy()
+        hits = rng.random(n) < 0.02
+        mut[hits] = rng.choice(np.frombuffer(b"ACGT", np.uint8), size=int(hits.sum()))
+        parts.append(mut)
+    for _ in range(300):
+        s = int(rng.integers(0, genome.size - k))
+        parts.append(genome[s:s + k] if rng.random() < 0.5 else wl.random_bases(rng, k))
+    letters = np.concatenate(parts)
+    rows = np.zeros(len(parts) + 1, dtype=np.uint64)
+    rows[1:] = np.cumsum([p.size for p in parts])
+    return letters, rows
+
+
+@pytest.mark.parametrize("k,p", [(31, 10), (31, 0), (31, 13), (5, 3), (5, 5), (32, 12), (12, 6)])
+@pytest.mark.parametrize("layout", [sg.SBWT_LAYOUT_LINES, sg.SBWT_LAYOUT_POPPY])
+def test_absent_run_skip_equals_per_kmer_search(cuda, k, p, layout):
+    """The right-to-left run walk with the absent-run skip answers exactly as the
+    per-k-mer search (skip off) and the oracle."""
+    rng = wl.rng_for(2000 + k * 17 + p)
+    genome = wl.random_bases(rng, 60_000)
+    built = sg.build_sbwt([genome.tobytes()], k)
+    letters, rows = _row_mixture(rng, genome, k)
+    ox = orc.OracleIndex(built.bits, built.n_bits)
+    want = ox.search_reads(letters, rows, k, p)
+    if k >= 12:
+        assert 0.05 < (want != orc.NOT_FOUND).mean() < 0.95
+    with sg.Index.from_bits(built.bits, built.n_bits, k=k, k_presearch=p) as ix:
+        ix.configure(layout, kmers_per_thread=0)
+        on = run_reads(ix, letters, rows, cuda)
+        ix.set_absent_skip(False)
+        off = run_reads(ix, letters, rows, cuda)
+        ix.set_absent_skip(True)
+        on2 = run_reads(ix, letters, rows, cuda, n_kmers=want.size // 2 + 7)
+    assert np.array_equal(on, want)
+    assert np.array_equal(off, want)
+    assert np.array_equal(on2, want[: want.size // 2 + 7])
+
+
+def test_absent_run_skip_default_param(cuda):
+    p = sg.default_params()
+    assert p.skip_absent_runs == 1
