@@ -60,8 +60,8 @@ def parse():
     ap.add_argument("--no-prefilter", action="store_true", help="skip the learned-prefilter leg")
     ap.add_argument("--no-autotune", action="store_true", help="skip the autotuned leg")
     ap.add_argument("--no-per-kmer", action="store_true", help="skip the leg that searches every k-mer")
-    ap.add_argument("--search-every-kmer", action="store_true",
-                    help="main leg without the absent-run skip (every k-mer searched, as the reference does)")
+    ap.add_argument("--search-mode", choices=["every", "skip", "stream"], default="stream",
+                    help="main leg: every k-mer searched (as the reference), absent-run skip, or skip + backward steps")
     ap.add_argument("--pf-queries", type=int, default=200_000_000)
     ap.add_argument("--pf-steps", type=int, default=20000)
     ap.add_argument("--workload", choices=["large", "batched", "pangenome"], default="large",
@@ -69,6 +69,8 @@ def parse():
                          "index; pangenome = 20 haplotypes of a 50 Mbp base")
     return ap.parse_args()
 
+
+MODES = {"every": 0, "skip": 1, "stream": 2}
 
 WORKLOADS = {
     "large": "large: 100 Mbp genome (41% GC) + 5% repeats, SBWT k=31, p=12, "
@@ -219,11 +221,13 @@ def cpu_reference(ox, letters, rows, k, p, budget_s, table):
     return ans.size / dt, ans, steps, nr, threads
 
 
-def searched_fraction(ans, steps, rows, k, p, max_rows=20000):
-    """Share of k-mers the run walk actually searches (right to left per read; a search that fails
-    after m letters settles k-m+1 k-mers), from per-k-mer oracle answers and step counts."""
+def walk_model(ans, steps, rows, k, p, stream, max_rows=20000):
+    """Share of k-mers the run walk searches from scratch, and share it reaches by a backward step
+    (right to left per read; a search that fails after m letters settles k-m+1 k-mers; with
+    `stream`, the k-mer left of a found one takes a backward step), from per-k-mer oracle answers
+    and step counts of the first `max_rows` reads."""
     import oracle as orc
-    searched = total = 0
+    searched = back = total = 0
     j0 = 0
     for r in range(min(rows.size - 1, max_rows)):
         n = int(rows[r + 1] - rows[r]) - k + 1
@@ -232,15 +236,23 @@ def searched_fraction(ans, steps, rows, k, p, max_rows=20000):
         if j0 + n > ans.size:
             break
         j = j0 + n - 1
+        have = False
         while j >= j0:
-            searched += 1
-            if ans[j] != orc.NOT_FOUND:
+            hit = ans[j] != orc.NOT_FOUND
+            if stream and have:
+                back += 1
+                have = hit
                 j -= 1
             else:
-                j -= k - min(max(p, p + int(steps[j])), k) + 1
+                searched += 1
+                if hit:
+                    have = True
+                    j -= 1
+                else:
+                    j -= k - min(max(p, p + int(steps[j])), k) + 1
         j0 += n
         total += n
-    return searched / max(total, 1)
+    return searched / max(total, 1), back / max(total, 1)
 
 
 def kernel_traffic(kernel, workload, n_kmers):
@@ -287,7 +299,7 @@ def main():
     prefix = os.path.join(tmpdir, "ix")
     if rank == 0:
         t = time.perf_counter()
-        built = sg.build_sbwt([x.tobytes() for x in seqs], k)
+        built = sg.build_sbwt([x.tobytes() for x in seqs], k, device=local_rank)  # the GPU builder
         build_s = time.perf_counter() - t
         paths = sg.write_index_files(prefix, built)
         n_columns = built.n_bits
@@ -299,9 +311,10 @@ def main():
     t = time.perf_counter()
     ix = sg.Index.load(*paths, k=k, k_presearch=p, device=local_rank, layout=layout,
                        kmers_per_thread=args.kpt, threads_per_kmer=args.tpk, threads_per_block=args.tpb,
-                       skip_absent_runs=0 if args.search_every_kmer else 1)
-    runs_form = args.kpt == 0 and not args.search_every_kmer and (args.tpk <= 1 or args.layout == "poppy")
-    kernel = "search_runs_kernel" if runs_form else ("search_queue_kernel" if args.kpt == 0 else "search_kernel")
+                       search_mode=MODES[args.search_mode])
+    runs_form = args.kpt == 0 and args.search_mode != "every" and (args.tpk <= 1 or args.layout == "poppy")
+    kernel = ("search_runs_kernel" + ("<stream>" if args.search_mode == "stream" else "<skip>") if runs_form
+              else ("search_queue_kernel" if args.kpt == 0 else "search_kernel"))
     load_s = time.perf_counter() - t
     info = ix.info()
 
@@ -354,7 +367,7 @@ def main():
         if not np.array_equal(got, ans):
             raise SystemExit(f"bench: {int((got != ans).sum())} of {ans.size} sampled answers differ from the oracle")
         mean_steps = float(steps.mean())
-        searched = searched_fraction(ans, steps, rows, k, p) if runs_form else 1.0
+        searched, back = walk_model(ans, steps, rows, k, p, args.search_mode == "stream") if runs_form else (1.0, 0.0)
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"first {nr} reads ({ans.size} k-mers) of the same batch, C restatement of the reference "
                          f"search (the reference has no CPU search), OpenMP schedule(dynamic,4096)"}
@@ -387,7 +400,7 @@ def main():
     per_kmer = None
     if runs_form and not args.no_per_kmer and rank == 0:
         ix.profile(True)
-        ix.set_absent_skip(False)
+        ix.set_search_mode(sg.SEARCH_EVERY_KMER)
         for _ in range(2):
             step()
         torch.cuda.synchronize(dev)
@@ -399,7 +412,7 @@ def main():
         ev1.record(stream)
         torch.cuda.synchronize(dev)
         tt = ev0.elapsed_time(ev1)
-        ix.set_absent_skip(True)
+        ix.set_search_mode(MODES[args.search_mode])
         got = d_ans[: ans.size].cpu().numpy().view(np.uint64)
         if not np.array_equal(got, ans):
             raise SystemExit("bench: per-k-mer answers differ from the oracle")
@@ -458,12 +471,12 @@ def main():
                 "l2": "inputs and outputs larger than L2 (letters %.2f GB, answers %.2f GB); no flush" % (
                     letters.nbytes / 1e9, n_kmers * 8 / 1e9),
                 "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                "index_build_s": round(build_s, 2), "index_load_s": round(load_s, 2),
+                "index_build_s": round(build_s, 2), "index_builder": "gpu (sbwt_build_gpu, incl. host copies)", "index_load_s": round(load_s, 2),
             },
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": f"of {peak_kind}",
                          "kernel": kernel, "kernel_ms": kern_ms, "bytes_per_kmer_model": b_kmer,
-                         "mean_steps": mean_steps, "searched_fraction": searched,
+                         "mean_steps": mean_steps, "searched_fraction": searched, "backward_step_fraction": back,
                          "dram_frac": (traffic / (kern_ms / 1e3) / 1e9 / peak) if traffic else None,
                          "traffic_source": tr["source"] if tr else None},
             "cpu_baseline": cpu,

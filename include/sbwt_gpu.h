@@ -56,12 +56,24 @@ typedef struct {
     uint32_t kmers_per_thread;   /* search kernel: 0 = one k-mer per lane fed from a per-warp queue
                                     (default); 1,2,3,4,6,8 = k-mer slots held in registers */
     uint32_t threads_per_kmer;   /* search kernel: lanes sharing one k-mer, 1|2|4 (0 = default) */
-    int32_t skip_absent_runs;    /* searches of reads with the queue-fed kernel: 1 (default) = walk each
-                                    read from right to left and, when a k-mer's search fails after m
-                                    letters, answer the k-m+1 k-mers that contain those m letters as
-                                    absent without searching them; 0 = search every k-mer.  The
-                                    answers are the same either way.  No reference counterpart. */
+    int32_t search_mode;         /* searches of reads with the queue-fed kernel (SBWT_SEARCH_*, default
+                                    SBWT_SEARCH_STREAM).  The answers are the same in every mode.
+                                    No reference counterpart. */
 } sbwt_params;
+
+/* Search modes for batches of reads (sbwt_params.search_mode, sbwt_set_search_mode).
+ * EVERY_KMER: every k-mer is searched from scratch, as the reference does.
+ * SKIP_ABSENT: each read is walked from right to left; when a k-mer's search
+ *   fails after m letters, those m letters are in no indexed k-mer, so the
+ *   k-m+1 k-mers containing them are answered absent without a search.
+ * STREAM: SKIP_ABSENT, and after a k-mer is found the k-mer one letter to its
+ *   left is reached by one backward step (a select and a look at the <= 5
+ *   nodes of one suffix group) instead of a new search.  Needs the line
+ *   layout's index size limit and one byte per column plus select samples,
+ *   built on the GPU when the mode is selected. */
+#define SBWT_SEARCH_EVERY_KMER 0
+#define SBWT_SEARCH_SKIP_ABSENT 1
+#define SBWT_SEARCH_STREAM 2
 
 /* Fills the defaults (k=30, p=12, SB=1024, poppy, no shuffles, device 0,
  * line layout).  No reference counterpart (the reference uses member
@@ -125,10 +137,17 @@ int sbwt_configure(sbwt_index *index, int32_t layout, uint32_t bits_in_superbloc
                    int32_t with_shuffles, uint32_t kmers_per_thread, uint32_t threads_per_kmer,
                    uint32_t threads_per_block);
 
-/* Turns the absent-run skip of sbwt_params.skip_absent_runs on (1) or off
- * (0) for later searches of reads on this index.  No reference counterpart:
- * the reference searches every k-mer (include/gpu/search_kernel.hpp:61-104). */
-int sbwt_set_absent_skip(sbwt_index *index, int32_t on);
+/* Selects the search mode (SBWT_SEARCH_*) for later searches of reads on this
+ * index, building the backward-step structures on first use of
+ * SBWT_SEARCH_STREAM.  No reference counterpart: the reference searches every
+ * k-mer (include/gpu/search_kernel.hpp:61-104). */
+int sbwt_set_search_mode(sbwt_index *index, int32_t mode);
+
+/* Copies the per-column node bytes of the backward step to the host (count =
+ * number of columns): bits 0-2 the first letter of the node's label (0 = $,
+ * 1..4 = A, C, G, T), bit 3 set on the first node of each group of nodes
+ * sharing their last k-1 letters.  For tests; no reference counterpart. */
+int sbwt_node_bytes_export(sbwt_index *index, uint8_t *out, uint64_t count);
 
 /* Sets the L2 fetch granularity (32, 64 or 128 bytes; cudaLimitMaxL2FetchGranularity)
  * of the index's device for this process, as the reference does before its
@@ -331,6 +350,14 @@ void sbwt_queries_free(sbwt_queries *q);
 int64_t sbwt_format_answers(const uint64_t *row_starts, uint64_t n_rows, uint32_t k, const uint64_t *answers,
                             char *out, uint64_t cap);
 
+/* The same text formatted on the GPU from device buffers: row_starts (n_rows
+ * + 1 letter offsets, as sbwt_search_reads takes them) and n_kmers answers.
+ * *bytes receives the text's length; with d_out == NULL nothing is written
+ * (size query), otherwise cap must be at least *bytes.  Synchronises
+ * `stream`.  Replaces the host loop of results_persister.hpp:82-95. */
+int sbwt_format_answers_device(const uint64_t *d_row_starts, uint64_t n_rows, uint32_t k, const uint64_t *d_answers,
+                               uint64_t n_kmers, char *d_out, uint64_t cap, uint64_t *bytes, void *stream);
+
 /* -------------------------------------------------------------- builder */
 
 /* Builds the plain-matrix SBWT of every k-mer of the given sequences
@@ -351,6 +378,14 @@ typedef struct {
 
 int sbwt_build(const uint8_t *seqs, const uint64_t *seq_starts, uint64_t n_seqs, uint32_t k, sbwt_built *out);
 void sbwt_build_free(sbwt_built *b);
+
+/* The same construction on GPU `device` (k-mer enumeration, radix sort, dummy
+ * nodes, bit-vector emit as kernels); its output equals sbwt_build's bit for
+ * bit and is released with sbwt_build_free.  No reference counterpart (the
+ * reference relies on an external construction tool, include/matrix_sbwt.hpp:
+ * 44-55). */
+int sbwt_build_gpu(const uint8_t *seqs, const uint64_t *seq_starts, uint64_t n_seqs, uint32_t k, int32_t device,
+                   sbwt_built *out);
 
 /* Writes vector c of a built index to `path` in the reference file format
  * (include/bit_vector.hpp:65-128). */

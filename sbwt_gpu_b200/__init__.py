@@ -23,14 +23,15 @@ from ._lib import (CLI_PATH, LIB_PATH, SBWT_CUM_POPPY, SBWT_LAYOUT_LINES, SBWT_L
 
 __all__ = [
     "Index", "Params", "SbwtError", "build_sbwt", "write_index_files", "read_queries", "format_answers",
-    "count_kmers", "read_queries_many", "default_params", "SBWT_POPPY", "SBWT_CUM_POPPY", "SBWT_LAYOUT_LINES", "SBWT_LAYOUT_POPPY",
-    "LIB_PATH", "CLI_PATH", "NOT_FOUND", "Prefilter", "mlp_params", "mlp_gradients", "mlp_logits", "MLP_PARAMS",
+    "count_kmers", "read_queries_many", "format_answers_device", "default_params", "SBWT_POPPY", "SBWT_CUM_POPPY", "SBWT_LAYOUT_LINES", "SBWT_LAYOUT_POPPY",
+    "LIB_PATH", "CLI_PATH", "NOT_FOUND", "SEARCH_EVERY_KMER", "SEARCH_SKIP_ABSENT", "SEARCH_STREAM", "Prefilter", "mlp_params", "mlp_gradients", "mlp_logits", "MLP_PARAMS",
 ]
 
 MLP_PARAMS = 256 * 128 + 256 + 256 * 256 + 256 + 256 + 1  # W1, b1, W2, b2, w3, b3
 
 NOT_FOUND = 0xFFFFFFFFFFFFFFFF  # answer of an absent k-mer (printed as -1)
 SBWT_KEEP = 0xFFFFFFFF  # sbwt_configure: leave the argument unchanged
+SEARCH_EVERY_KMER, SEARCH_SKIP_ABSENT, SEARCH_STREAM = 0, 1, 2  # sbwt_params.search_mode
 
 
 def default_params(**kw):
@@ -143,9 +144,17 @@ class Index:
         check(lib.sbwt_configure(self._h, layout, bits_in_superblock, rank_structure, int(with_shuffles),
                                  kmers_per_thread, threads_per_kmer, threads_per_block))
 
-    def set_absent_skip(self, on):
-        """Absent-run skip for searches of reads (on by default; answers are the same either way)."""
-        check(lib.sbwt_set_absent_skip(self._h, 1 if on else 0))
+    def set_search_mode(self, mode):
+        """SEARCH_EVERY_KMER, SEARCH_SKIP_ABSENT or SEARCH_STREAM (default) for searches of reads;
+        the answers are the same in every mode."""
+        check(lib.sbwt_set_search_mode(self._h, int(mode)))
+
+    def node_bytes(self):
+        """Per-column node bytes of the backward step: first letter (0 = $, 1..4 = ACGT) | 8 on group starts."""
+        n = self.info()["n_bits"]
+        out = np.empty(n, dtype=np.uint8)
+        check(lib.sbwt_node_bytes_export(self._h, _ptr(out), n))
+        return out
 
     def autotune(self, d_letters, d_row_starts, d_answers, n_kmers, tune_p=False, tune_poppy=False):
         """Times candidate launch shapes on a device sample, keeps the fastest; returns the JSON report."""
@@ -319,11 +328,15 @@ def _as_letters_and_starts(seqs):
     return letters, starts
 
 
-def build_sbwt(seqs, k):
-    """Builds the plain-matrix SBWT of all k-mers of ``seqs`` (list of str/bytes, or (letters, starts))."""
+def build_sbwt(seqs, k, device=None):
+    """Builds the plain-matrix SBWT of all k-mers of ``seqs`` (list of str/bytes, or (letters, starts)):
+    on the host, or on GPU ``device`` when given (same bits)."""
     letters, starts = _as_letters_and_starts(seqs)
     b = Built()
-    check(lib.sbwt_build(_ptr(letters), _ptr(starts), starts.size - 1, int(k), byref(b)))
+    if device is None:
+        check(lib.sbwt_build(_ptr(letters), _ptr(starts), starts.size - 1, int(k), byref(b)))
+    else:
+        check(lib.sbwt_build_gpu(_ptr(letters), _ptr(starts), starts.size - 1, int(k), int(device), byref(b)))
     try:
         bits = [np.ctypeslib.as_array(b.bits[c], shape=(b.n_words,)).copy() for c in range(4)]
     finally:
@@ -388,3 +401,17 @@ def format_answers(row_starts, k, answers):
     if got < 0:
         raise SbwtError("format buffer too small")
     return buf.raw[:got]
+
+
+def format_answers_device(d_row_starts, k, d_answers, stream=None):
+    """The same text formatted on the GPU from device tensors (int64 row starts and answers); bytes."""
+    import torch
+    n_rows = int(d_row_starts.numel()) - 1
+    nk = int(d_answers.numel())
+    nbytes = c_uint64(0)
+    check(lib.sbwt_format_answers_device(_ptr(d_row_starts), n_rows, int(k), _ptr(d_answers), nk, None, 0,
+                                         byref(nbytes), _stream_ptr(stream)))
+    out = torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=d_answers.device)
+    check(lib.sbwt_format_answers_device(_ptr(d_row_starts), n_rows, int(k), _ptr(d_answers), nk, _ptr(out),
+                                         int(out.numel()), byref(nbytes), _stream_ptr(stream)))
+    return bytes(out[: int(nbytes.value)].cpu().numpy())

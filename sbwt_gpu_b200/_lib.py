@@ -32,7 +32,7 @@ class Params(ctypes.Structure):
         ("layout", c_int32),
         ("kmers_per_thread", c_uint32),
         ("threads_per_kmer", c_uint32),
-        ("skip_absent_runs", c_int32),
+        ("search_mode", c_int32),
     ]
 
 
@@ -118,7 +118,8 @@ SIGNATURES = {
     "sbwt_presearch_export": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64]),
     "sbwt_rank_export": (c_int, [c_void_p, c_uint32, c_int32, c_int, c_void_p, c_uint64, c_void_p, c_uint64]),
     "sbwt_configure": (c_int, [c_void_p, c_int32, c_uint32, c_int32, c_int32, c_uint32, c_uint32, c_uint32]),
-    "sbwt_set_absent_skip": (c_int, [c_void_p, c_int32]),
+    "sbwt_set_search_mode": (c_int, [c_void_p, c_int32]),
+    "sbwt_node_bytes_export": (c_int, [c_void_p, c_void_p, c_uint64]),
     "sbwt_search_packed": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_void_p]),
     "sbwt_pack": (c_int, [c_void_p, c_uint64, c_void_p, c_void_p]),
     "sbwt_search_reads": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_void_p, c_void_p, c_uint64,
@@ -150,6 +151,9 @@ SIGNATURES = {
     "sbwt_queries_free": (None, [POINTER(Queries)]),
     "sbwt_format_answers": (c_int64, [c_void_p, c_uint64, c_uint32, c_void_p, c_void_p, c_uint64]),
     "sbwt_build": (c_int, [c_void_p, c_void_p, c_uint64, c_uint32, POINTER(Built)]),
+    "sbwt_format_answers_device": (c_int, [c_void_p, c_uint64, c_uint32, c_void_p, c_uint64, c_void_p, c_uint64,
+                                           POINTER(c_uint64), c_void_p]),
+    "sbwt_build_gpu": (c_int, [c_void_p, c_void_p, c_uint64, c_uint32, c_int32, POINTER(Built)]),
     "sbwt_build_free": (None, [POINTER(Built)]),
     "sbwt_write_bitvector": (c_int, [c_char_p, c_void_p, c_uint64]),
 }

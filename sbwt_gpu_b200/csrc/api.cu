@@ -74,6 +74,9 @@ int use_device(int device) {
 int validate_params(const sbwt_params *p) {
     if (p->k < 3 || p->k > 32) return set_error("The value of k must be at least 3 and at most 32.");
     if (p->k_presearch > p->k) return set_error("presearch depth %u exceeds k = %u", p->k_presearch, p->k);
+    if (p->search_mode != SBWT_SEARCH_EVERY_KMER && p->search_mode != SBWT_SEARCH_SKIP_ABSENT &&
+        p->search_mode != SBWT_SEARCH_STREAM)
+        return set_error("unknown search mode %d", p->search_mode);
     return 0;
 }
 
@@ -88,7 +91,7 @@ void apply_shape(sbwt_index *ix, const sbwt_params *p) {
     sh.sb = p->bits_in_superblock;
     sh.kind = p->rank_structure;
     sh.shuffles = p->with_shuffles;
-    sh.skip = p->skip_absent_runs ? 1 : 0;
+    sh.mode = p->search_mode;
 }
 
 // Shared tail of the two index constructors: `words[c]` hold ceil(n/64)
@@ -142,6 +145,7 @@ int finish_index(sbwt_index *ix, const u64 *const words[4], const sbwt_params *p
     apply_shape(ix, prm);
     if (ix->shape.layout == SBWT_LAYOUT_LINES && !ix->lines_ok) ix->shape.layout = SBWT_LAYOUT_POPPY;
     SBWT_TRY(sbwt::run_presearch(ix, prm->k_presearch, s));
+    if (ix->shape.mode == SBWT_SEARCH_STREAM && ix->lines_ok) SBWT_TRY(sbwt::build_stream(ix, s));
     SBWT_CHECK_CUDA(cudaDeviceSynchronize());
     return 0;
 }
@@ -223,7 +227,7 @@ extern "C" int sbwt_params_default(sbwt_params *p) {
     p->layout = SBWT_LAYOUT_LINES;
     p->kmers_per_thread = 0;
     p->threads_per_kmer = 0;
-    p->skip_absent_runs = 1;
+    p->search_mode = SBWT_SEARCH_STREAM;
     return 0;
 }
 
@@ -279,6 +283,8 @@ extern "C" void sbwt_index_free(sbwt_index *ix) {
     cudaFree(ix->d_L12);
     cudaFree(ix->d_pre);
     cudaFree(ix->d_scan);
+    cudaFree(ix->d_node);
+    cudaFree(ix->d_sel);
     for (int i = 0; i < 2; i++) {
         ix->ws[i].release();
         if (ix->pipe_stream[i]) cudaStreamDestroy(ix->pipe_stream[i]);
@@ -357,10 +363,14 @@ extern "C" int sbwt_configure(sbwt_index *ix, int32_t layout, uint32_t sb, int32
     return 0;
 }
 
-extern "C" int sbwt_set_absent_skip(sbwt_index *ix, int32_t on) {
+extern "C" int sbwt_set_search_mode(sbwt_index *ix, int32_t mode) {
     clear_error();
     if (!ix) return set_error("index is NULL");
-    ix->shape.skip = on ? 1 : 0;
+    if (mode != SBWT_SEARCH_EVERY_KMER && mode != SBWT_SEARCH_SKIP_ABSENT && mode != SBWT_SEARCH_STREAM)
+        return set_error("unknown search mode %d", mode);
+    SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
+    if (mode == SBWT_SEARCH_STREAM && ix->lines_ok) SBWT_TRY(build_stream(ix, 0));
+    ix->shape.mode = mode;
     return 0;
 }
 
@@ -384,6 +394,8 @@ SearchArgs base_args(const sbwt_index *ix, bool rows) {
     a.k = ix->k;
     a.chunk = search_chunk(ix, rows);
     a.runs = rows && runs_form(ix);
+    a.stream = a.runs && stream_form(ix);
+    if (a.stream) a.sv = stream_view(ix);
     return a;
 }
 
@@ -412,7 +424,7 @@ int search_rows_device(sbwt_index *ix, Workspace &w, const uint8_t *d_letters, u
         const KernelShape &sh = ix->shape;
         const uint64_t key[12] = {(uint64_t)d_letters, n_letters, (uint64_t)d_rows, n_rows, (uint64_t)d_answers,
                                   (uint64_t)d_member, n_kmers, (uint64_t)s, ix->gen,
-                                  ((uint64_t)sh.layout << 48) | ((uint64_t)sh.skip << 40) | ((uint64_t)sh.kpt << 32) |
+                                  ((uint64_t)sh.layout << 48) | ((uint64_t)sh.mode << 40) | ((uint64_t)sh.kpt << 32) |
                                       ((uint64_t)sh.tpk << 16) | sh.tpb,
                                   (uint64_t)w.words ^ (uint64_t)w.kstart, (uint64_t)w.chunk_row ^ (uint64_t)w.counter};
         if (w.graph && std::memcmp(key, w.graph_key, sizeof key) == 0) {
@@ -465,15 +477,17 @@ int enqueue_rows(sbwt_index *ix, Workspace &w, SearchArgs &a, const uint8_t *d_l
     a.answers = d_answers;
     a.n_kmers = n_kmers;
     a.counter = w.counter;
+    a.member = a.runs ? d_member : nullptr;  // the run-walking kernel writes the bitmap itself
+    const bool member_pass = d_member && !a.runs;
     uint32_t blocks = 0;
     SBWT_TRY(launch_search(ix, a, s, &blocks));
     if (prof) SBWT_CHECK_CUDA(cudaEventRecord(ix->prof_ev[3], s));
-    if (d_member) SBWT_TRY(launch_member_bits(d_answers, n_kmers, d_member, s));
+    if (member_pass) SBWT_TRY(launch_member_bits(d_answers, n_kmers, d_member, s));
     if (prof) {
         SBWT_CHECK_CUDA(cudaEventRecord(ix->prof_ev[4], s));
-        ix->prof_launches = 1 + 3 + 1 + 1 + (d_member ? 1 : 0);
+        ix->prof_launches = 1 + 3 + 1 + 1 + (member_pass ? 1 : 0);
         ix->prof_blocks = blocks;
-        ix->prof_member = d_member != nullptr;
+        ix->prof_member = member_pass;
     }
     return 0;
 }

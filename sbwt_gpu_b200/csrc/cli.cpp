@@ -11,6 +11,7 @@
 //               [--device-set-limit-presearch=64] [--device-set-limit-search=64]
 //               [--do-not-store-results] [--layout=lines|poppy]
 //               [--kmers-per-thread=N] [--threads-per-kmer=1|2|4]
+//               [--search-mode=every|skip|stream]
 //
 // Differences from the reference: errors return a non-zero exit status
 // (the reference always returns 0, src/search.cpp:14-25); --rank-structure=
@@ -43,7 +44,7 @@ void print_help() {
                  "       [--rank-structure=poppy|cum-poppy] [--with-shuffles] [--threads-per-block=N]\n"
                  "       [--device-set-limit-presearch=32|64|128] [--device-set-limit-search=32|64|128]\n"
                  "       [--do-not-store-results] [--layout=lines|poppy] [--kmers-per-thread=N]\n"
-                 "       [--threads-per-kmer=1|2|4]\n");
+                 "       [--threads-per-kmer=1|2|4] [--search-mode=every|skip|stream]\n");
 }
 
 struct Options {
@@ -83,7 +84,9 @@ int parse(int argc, char **argv, Options &o) {
             std::fprintf(stderr, "Ignoring %s.\n", s.c_str());
         } else if (s == "--layout=lines") o.p.layout = SBWT_LAYOUT_LINES;
         else if (s == "--layout=poppy") o.p.layout = SBWT_LAYOUT_POPPY;
-        else if (s == "--search-every-kmer") o.p.skip_absent_runs = 0;
+        else if (s == "--search-mode=every") o.p.search_mode = SBWT_SEARCH_EVERY_KMER;
+        else if (s == "--search-mode=skip") o.p.search_mode = SBWT_SEARCH_SKIP_ABSENT;
+        else if (s == "--search-mode=stream") o.p.search_mode = SBWT_SEARCH_STREAM;
         else if (std::regex_match(s, m, sb_re)) o.p.bits_in_superblock = (uint32_t)std::stoul(m[1]);
         else if (std::regex_match(s, m, lp_re)) o.limit_presearch = std::stoi(m[1]);
         else if (std::regex_match(s, m, ls_re)) o.limit_search = std::stoi(m[1]);
@@ -128,6 +131,83 @@ int parse(int argc, char **argv, Options &o) {
     return 0;
 }
 
+// Searches the reads of q in batches of at most kBatchLetters letters and
+// writes the reference's text for them to `out`.
+constexpr uint64_t kBatchLetters = 1ull << 28;
+
+int search_and_write(sbwt_index *ix, const sbwt_queries &q, uint32_t k, FILE *out) {
+    uint8_t *d_letters = nullptr;
+    uint64_t *d_rows = nullptr, *d_ans = nullptr;
+    char *d_text = nullptr, *h_text = nullptr;
+    uint64_t cap_l = 0, cap_r = 0, cap_a = 0, cap_t = 0;
+    std::vector<uint64_t> rows;
+    int rc = 0;
+    auto grow = [](auto *&p, uint64_t &cap, uint64_t need) {
+        if (need <= cap) return true;
+        cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        if (cudaMalloc((void **)&p, need * sizeof(*p)) != cudaSuccess) return false;
+        cap = need;
+        return true;
+    };
+    uint64_t r0 = 0;
+    while (rc == 0 && r0 < q.n_rows) {
+        // rows [r0, r1): at least one, at most kBatchLetters letters unless one read is longer
+        uint64_t r1 = r0 + 1;
+        while (r1 < q.n_rows && q.row_starts[r1 + 1] - q.row_starts[r0] <= kBatchLetters) r1++;
+        const uint64_t base = q.row_starts[r0], nl = q.row_starts[r1] - base, nr = r1 - r0;
+        rows.resize(nr + 1);
+        uint64_t nk = 0;
+        for (uint64_t r = 0; r <= nr; r++) {
+            rows[r] = q.row_starts[r0 + r] - base;
+            if (r < nr) {
+                const uint64_t len = q.row_starts[r0 + r + 1] - q.row_starts[r0 + r];
+                nk += len >= k ? len - k + 1 : 0;
+            }
+        }
+        uint64_t bytes = 0;
+        if (!grow(d_letters, cap_l, nl + 1) || !grow(d_rows, cap_r, nr + 1) || !grow(d_ans, cap_a, nk + 1)) {
+            rc = 1;
+            break;
+        }
+        if (cudaMemcpy(d_letters, q.letters + base, nl, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(d_rows, rows.data(), (nr + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice) != cudaSuccess) {
+            rc = 1;
+            break;
+        }
+        if (nk && sbwt_search_reads(ix, d_letters, nl, d_rows, nr, d_ans, nullptr, nk, nullptr)) {
+            rc = 1;
+            break;
+        }
+        if (sbwt_format_answers_device(d_rows, nr, k, d_ans, nk, nullptr, 0, &bytes, nullptr) ||
+            !grow(d_text, cap_t, bytes + 1)) {
+            rc = 1;
+            break;
+        }
+        if (sbwt_format_answers_device(d_rows, nr, k, d_ans, nk, d_text, cap_t, &bytes, nullptr)) {
+            rc = 1;
+            break;
+        }
+        cudaFreeHost(h_text);
+        h_text = nullptr;
+        if (cudaMallocHost((void **)&h_text, bytes + 1) != cudaSuccess ||
+            cudaMemcpy(h_text, d_text, bytes, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            std::fwrite(h_text, 1, bytes, out) != bytes) {
+            rc = 1;
+            break;
+        }
+        r0 = r1;
+    }
+    std::fflush(out);
+    cudaFree(d_letters);
+    cudaFree(d_rows);
+    cudaFree(d_ans);
+    cudaFree(d_text);
+    cudaFreeHost(h_text);
+    return rc;
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
@@ -164,30 +244,31 @@ int main(int argc, char **argv) {
         return 1;
     }
     const double ms_read = ms_since(t1);
-    std::vector<uint64_t> answers(q.n_kmers ? q.n_kmers : 1);
+    int rc = 0;
     auto t2 = std::chrono::steady_clock::now();
-    if (sbwt_search_reads_host(ix, q.letters, q.n_letters, q.row_starts, q.n_rows, answers.data(), q.n_kmers)) {
-        std::fprintf(stderr, "%s\n", sbwt_last_error());
-        sbwt_queries_free(&q);
-        sbwt_index_free(ix);
-        return 1;
+    if (o.store) {
+        // batches of whole reads: letters + offsets to the device, search, text formatted on the
+        // device (sbwt_format_answers_device), text back and written in read order
+        if (search_and_write(ix, q, o.p.k, stdout)) {
+            const char *msg = sbwt_last_error();
+            std::fprintf(stderr, "%s\n", msg && *msg ? msg : cudaGetErrorString(cudaGetLastError()));
+            rc = 1;
+        }
+    } else {
+        std::vector<uint64_t> answers(q.n_kmers ? q.n_kmers : 1);
+        if (sbwt_search_reads_host(ix, q.letters, q.n_letters, q.row_starts, q.n_rows, answers.data(), q.n_kmers)) {
+            std::fprintf(stderr, "%s\n", sbwt_last_error());
+            rc = 1;
+        }
     }
     const double ms_search = ms_since(t2);
     std::fprintf(stderr, "Reading the query file: %f ms.\n", ms_read);
-    std::fprintf(stderr, "Search (host to device, pack, search, device to host): %f ms.\n", ms_search);
+    std::fprintf(stderr, "Search (host to device, pack, search%s, device to host): %f ms.\n",
+                 o.store ? ", answer text, writing" : "", ms_search);
     std::fprintf(stderr, "Number of k-mers queried: %llu\n", (unsigned long long)q.n_kmers);
     if (q.n_kmers)
         std::fprintf(stderr, "Total per query: %f ns.\n", ms_search * 1e6 / (double)q.n_kmers);
-    int rc = 0;
-    if (o.store) {
-        const int64_t bytes = sbwt_format_answers(q.row_starts, q.n_rows, o.p.k, answers.data(), nullptr, 0);
-        std::vector<char> text((size_t)bytes + 1);
-        sbwt_format_answers(q.row_starts, q.n_rows, o.p.k, answers.data(), text.data(), (uint64_t)text.size());
-        if (std::fwrite(text.data(), 1, (size_t)bytes, stdout) != (size_t)bytes) rc = 1;
-        std::fflush(stdout);
-    } else {
-        std::fprintf(stderr, "The results are not stored to the file.\n");
-    }
+    if (!o.store) std::fprintf(stderr, "The results are not stored to the file.\n");
     sbwt_queries_free(&q);
     sbwt_index_free(ix);
     return rc;

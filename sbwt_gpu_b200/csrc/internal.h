@@ -6,6 +6,7 @@
 
 #include "sbwt_gpu.h"
 #include "common.h"
+#include "stream.cuh"
 
 namespace sbwt {
 
@@ -39,6 +40,9 @@ struct SearchArgs {
     unsigned long long *counter;  // work-stealing cursor (zeroed before launch)
     u32 chunk;                    // k-mers per grab; with `runs`, k-mers per window of chunk_row
     u32 runs;                     // read mode: walk runs right to left with the absent-run skip
+    u32 stream;                   // with `runs`: backward steps from a found k-mer (needs sv)
+    dev::StreamView sv;           // select samples + node bytes (stream.cuh)
+    uint32_t *member;             // with `runs`: membership bitmap written by the search kernel, or NULL
     // k-mer list mode: k-mer j is kmer_list[j] (MSB-first word)
     const u64 *kmer_list;
     // learned prefilter: skip k-mer j if logits[j] < tau and the Bloom filter rejects it
@@ -58,7 +62,7 @@ struct KernelShape {
     u32 sb = 1024;
     int kind = SBWT_POPPY;
     int shuffles = 0;
-    int skip = 1;  // read mode, queue-fed form: absent-run skip (search_runs_kernel)
+    int mode = SBWT_SEARCH_STREAM;  // batches of reads with the queue-fed form (sbwt_params.search_mode)
 };
 
 // Device buffers of one in-flight search (grow-only).
@@ -107,6 +111,11 @@ struct sbwt_index {
     uint32_t p = 0;
     void *d_pre = nullptr;
     bool pre64 = false;
+    // backward-step structures (stream.cu): node bytes and select samples
+    uint8_t *d_node = nullptr;
+    uint32_t *d_sel = nullptr;
+    uint32_t sel_off[4] = {0, 0, 0, 0}, sel_n[4] = {0, 0, 0, 0};
+    bool stream_ok = false;
     // launch shape
     sbwt::KernelShape shape;
     // scan block sums of the rank builds
@@ -146,6 +155,10 @@ int launch_chunk_rows(const uint64_t *d_kstart, uint64_t n_rows, uint64_t n_kmer
                       uint32_t *d_chunk_row, cudaStream_t s);
 int launch_member_bits(const uint64_t *d_answers, uint64_t n, uint32_t *d_bits, cudaStream_t s);
 
+// stream.cu
+int build_stream(sbwt_index *ix, cudaStream_t s);
+dev::StreamView stream_view(const sbwt_index *ix);
+
 // api.cu
 int search_rows_device(sbwt_index *ix, Workspace &w, const uint8_t *d_letters, u64 n_letters, const u64 *d_rows,
                        u64 n_rows, u64 *d_answers, uint32_t *d_member, u64 n_kmers, cudaStream_t s);
@@ -154,9 +167,11 @@ template <class T> int grow_host(T *&p, size_t &cap, size_t need);
 
 // search.cu
 int launch_search(const sbwt_index *ix, SearchArgs &a, cudaStream_t s, uint32_t *launched_blocks);
-// Whether a batch of reads searched with the index's current shape runs the
-// run-walking kernel with the absent-run skip.
+// Whether a batch of reads searched with the index's current shape and mode
+// runs the run-walking kernel (absent-run skip), and whether it also takes
+// backward steps.
 bool runs_form(const sbwt_index *ix);
+bool stream_form(const sbwt_index *ix);
 // Work granularity of a launch: k-mers per grab, or for the run-walking form
 // k-mers per window of the row table.  `rows`: a batch of reads.
 u32 search_chunk(const sbwt_index *ix, bool rows);

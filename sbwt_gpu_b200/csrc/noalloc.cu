@@ -106,6 +106,9 @@ extern "C" int sbwt_search_reads_noalloc(sbwt_index *ix, const uint8_t *d_letter
     a.k = ix->k;
     a.chunk = chunk;
     a.runs = runs_form(ix);
+    a.stream = a.runs && stream_form(ix);
+    if (a.stream) a.sv = stream_view(ix);
+    a.member = a.runs ? d_member_bits : nullptr;
     a.words = words;
     a.row_starts = d_row_starts;
     a.kstart = kstart;
@@ -116,6 +119,6 @@ extern "C" int sbwt_search_reads_noalloc(sbwt_index *ix, const uint8_t *d_letter
     a.n_kmers = n_kmers;
     a.counter = counter;  // launch_search clears it on the stream before the kernel
     SBWT_TRY(launch_search(ix, a, s, nullptr));
-    if (d_member_bits) SBWT_TRY(launch_member_bits(d_answers, n_kmers, d_member_bits, s));
+    if (d_member_bits && !a.runs) SBWT_TRY(launch_member_bits(d_answers, n_kmers, d_member_bits, s));
     return 0;
 }

@@ -342,12 +342,18 @@ __global__ void __launch_bounds__(128) search_queue_kernel(const R rk, const Sea
 // k-mers at once.  Their answers are the ~0 written when the run's window
 // was taken, so every answer equals the reference's per-k-mer search.
 //
+// With STREAM, a found k-mer's node also gives the node of the k-mer one
+// letter to its left by one backward step (stream.cuh) instead of a search
+// (presearch entry + k-p rank-pair steps); a failed backward step means that
+// k-mer is absent, and the next one is searched again.
+//
 // Work split: a warp takes 32 windows of kWin consecutive k-mer indices from
-// the global cursor and writes ~0 to all their answers (coalesced).  Each
-// lane cuts its window at row ends into runs and enqueues one run per fill
-// into the warp's shared-memory queue; an idle lane pops a run.  Every loop
-// iteration a lane either starts its run's next k-mer (letters + presearch
-// entry, followed by its first step) or takes one rank-pair step.
+// the global cursor and writes ~0 to all their answers (coalesced), and zero
+// to their membership words.  Each lane cuts its window at row ends into runs
+// and enqueues one run per fill into the warp's shared-memory queue; an idle
+// lane pops a run.  Every loop iteration a lane either starts its run's next
+// k-mer (backward step, or letters + presearch entry followed by its first
+// rank-pair step) or takes one rank-pair step.
 
 constexpr u32 kWin = 32;            // k-mers per window (granularity of chunk_row)
 constexpr u32 kStart = 0xfffffffeu; // lane state: start the run's current k-mer
@@ -358,7 +364,7 @@ struct RunEntry {
     u32 len;  // k-mers in the run, 1..kWin
 };
 
-template <class R>
+template <class R, bool STREAM>
 __global__ void __launch_bounds__(128) search_runs_kernel(const R rk, const SearchArgs a) {
     static_assert(sizeof(typename R::IT) == 4, "the run form serves 32-bit intervals");
     __shared__ RunEntry queue[kQueueWarps][kQueue];
@@ -370,6 +376,7 @@ __global__ void __launch_bounds__(128) search_runs_kernel(const R rk, const Sear
     const u32 rootR = (u32)(a.C[4] - 1ull);
     const PT *pre = reinterpret_cast<const PT *>(a.pre);
     const u64 n_eff = min(a.n_kmers, a.kstart[a.n_rows]);
+    uint32_t *const member = a.member;
     RunEntry *q = queue[warp];
 
     u32 head = 0, tail = 0;  // warp-uniform
@@ -378,6 +385,7 @@ __global__ void __launch_bounds__(128) search_runs_kernel(const R rk, const Sear
     u64 kmer = 0, J = 0, pos = 0;  // current k-mer of this lane's run
     u32 left = 0;                  // k-mers of the run left of J
     u32 L = 0, Rr = 0, I = kDone;
+    u32 V = dev::kNoNode;          // STREAM: node of the k-mer right of J (found), or kNoNode
 
     for (;;) {
         // ---- fill: new windows once every lane's window is cut, then one run per lane
@@ -393,8 +401,12 @@ __global__ void __launch_bounds__(128) search_runs_kernel(const R rk, const Sear
                     for (u64 t = base + lane; t < end; t += 32u) a.answers[t] = ~0ull;
                     pj = min((u64)base + (u64)lane * kWin, end);
                     pe = min(pj + kWin, end);
-                    if (pj < pe) prow = a.chunk_row[pj / kWin];
+                    if (pj < pe) {
+                        prow = a.chunk_row[pj / kWin];
+                        if (member) member[pj / 32u] = 0u;  // kWin = 32: one word per window
+                    }
                 }
+                __syncwarp();
             }
             if (more) {
                 const bool emit = pj < pe;
@@ -426,31 +438,41 @@ __global__ void __launch_bounds__(128) search_runs_kernel(const R rk, const Sear
             J = e.j;
             left = e.len - 1u;
             I = kStart;
+            V = dev::kNoNode;
         }
         head += take;
         __syncwarp();
-        // ---- start: letters (search_kernel.hpp:66-68) and presearch entry (:71-82)
-        u32 adv = 0;  // k-mers settled at and left of J
+        u32 adv = 0;      // k-mers settled at and left of J
+        u32 found = ~0u;  // node of k-mer J if found now
         if (I == kStart) {
-            const u64 b = min(pos, a.max_pos) << 1;
-            const u64 w0 = a.words[b >> 6], w1 = a.words[(b >> 6) + 1];
-            const u32 sh = (u32)(b & 63u);
-            kmer = (w0 << sh) | (shr_clamp(w1, 63u - sh) >> 1);
-            if (p) {
-                const PT e = pre[kmer >> (64u - 2u * p)];
-                L = e.x;
-                Rr = e.y;
-            } else {
-                L = 0;
-                Rr = rootR;
-            }
-            if (L > Rr) {
-                adv = k - p + 1u;  // x[J, J+p) is in no indexed k-mer
-            } else if (p >= k) {
-                a.answers[J] = (u64)L;
+            if (STREAM && V != dev::kNoNode) {
+                // ---- backward step: k-mer J = x[J] . (first k-1 letters of k-mer J+1)
+                const u32 letter = (u32)(a.words[pos >> 5] >> (62u - 2u * (u32)(pos & 31u))) & 3u;
+                const u32 u = a.sv.back_step(V, letter);
                 adv = 1;
+                if (u != dev::kNoNode) found = u;
             } else {
-                I = p;
+                // ---- start: letters (search_kernel.hpp:66-68) and presearch entry (:71-82)
+                const u64 b = min(pos, a.max_pos) << 1;
+                const u64 w0 = a.words[b >> 6], w1 = a.words[(b >> 6) + 1];
+                const u32 sh = (u32)(b & 63u);
+                kmer = (w0 << sh) | (shr_clamp(w1, 63u - sh) >> 1);
+                if (p) {
+                    const PT e = pre[kmer >> (64u - 2u * p)];
+                    L = e.x;
+                    Rr = e.y;
+                } else {
+                    L = 0;
+                    Rr = rootR;
+                }
+                if (L > Rr) {
+                    adv = k - p + 1u;  // x[J, J+p) is in no indexed k-mer
+                } else if (p >= k) {
+                    found = L;
+                    adv = 1;
+                } else {
+                    I = p;
+                }
             }
         }
         // ---- one rank-pair step (:84-96)
@@ -463,11 +485,16 @@ __global__ void __launch_bounds__(128) search_runs_kernel(const R rk, const Sear
             if (L > Rr) {
                 adv = k - I + 1u;  // x[J, J+I) is in no indexed k-mer
             } else if (I == k) {
-                a.answers[J] = (u64)L;
+                found = L;
                 adv = 1;
             }
         }
+        if (found != ~0u) {
+            a.answers[J] = (u64)found;
+            if (member) atomicOr(member + (J >> 5), 1u << (J & 31u));
+        }
         if (adv) {
+            if (STREAM) V = found != ~0u ? found : dev::kNoNode;
             if (adv > left) {
                 I = kDone;
             } else {
@@ -498,7 +525,8 @@ int launch_one(const R &rk, SearchArgs &a, const sbwt_index *ix, cudaStream_t s,
 
 template <class R>
 int launch_queue(const R &rk, SearchArgs &a, const sbwt_index *ix, cudaStream_t s, u32 *blocks_out) {
-    auto kern = a.runs ? search_runs_kernel<R> : search_queue_kernel<R>;
+    auto kern = a.runs ? (a.stream ? search_runs_kernel<R, true> : search_runs_kernel<R, false>)
+                       : search_queue_kernel<R>;
     int per_sm = 0;
     SBWT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, 0));
     if (per_sm < 1) per_sm = 1;
@@ -554,10 +582,14 @@ int poppy_sb(const sbwt_index *ix, SearchArgs &a, cudaStream_t s, const KernelSh
 
 bool runs_form(const sbwt_index *ix) {
     const KernelShape &sh = ix->shape;
-    if (!sh.skip || sh.kpt != 0) return false;
+    if (sh.mode == SBWT_SEARCH_EVERY_KMER || sh.kpt != 0) return false;
     if (sh.layout == SBWT_LAYOUT_LINES) return ix->lines_ok && sh.tpk == 1;
     // poppy: the queue-fed forms are the 32-bit single-lane ones
     return ix->n < (1ull << 32) && !(sh.shuffles && (ix->sb == 1024 || ix->sb == 2048));
+}
+
+bool stream_form(const sbwt_index *ix) {
+    return runs_form(ix) && ix->shape.mode == SBWT_SEARCH_STREAM && ix->stream_ok;
 }
 
 u32 search_chunk(const sbwt_index *ix, bool rows) {

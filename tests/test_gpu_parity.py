@@ -366,11 +366,11 @@ def _row_mixture(rng, genome, k):
     return letters, rows
 
 
-@pytest.mark.parametrize("k,p", [(31, 10), (31, 0), (31, 13), (5, 3), (5, 5), (32, 12), (12, 6)])
+@pytest.mark.parametrize("k,p", [(31, 10), (31, 0), (31, 13), (5, 3), (5, 5), (32, 12), (12, 6), (3, 2)])
 @pytest.mark.parametrize("layout", [sg.SBWT_LAYOUT_LINES, sg.SBWT_LAYOUT_POPPY])
-def test_absent_run_skip_equals_per_kmer_search(cuda, k, p, layout):
-    """The right-to-left run walk with the absent-run skip answers exactly as the
-    per-k-mer search (skip off) and the oracle."""
+def test_run_walk_modes_equal_per_kmer_search(cuda, k, p, layout):
+    """The right-to-left run walk (absent-run skip, and skip + backward steps) answers
+    exactly as the per-k-mer search and the oracle, bitmap included."""
     rng = wl.rng_for(2000 + k * 17 + p)
     genome = wl.random_bases(rng, 60_000)
     built = sg.build_sbwt([genome.tobytes()], k)
@@ -379,18 +379,51 @@ def test_absent_run_skip_equals_per_kmer_search(cuda, k, p, layout):
     want = ox.search_reads(letters, rows, k, p)
     if k >= 12:
         assert 0.05 < (want != orc.NOT_FOUND).mean() < 0.95
+    got = {}
     with sg.Index.from_bits(built.bits, built.n_bits, k=k, k_presearch=p) as ix:
         ix.configure(layout, kmers_per_thread=0)
-        on = run_reads(ix, letters, rows, cuda)
-        ix.set_absent_skip(False)
-        off = run_reads(ix, letters, rows, cuda)
-        ix.set_absent_skip(True)
-        on2 = run_reads(ix, letters, rows, cuda, n_kmers=want.size // 2 + 7)
-    assert np.array_equal(on, want)
-    assert np.array_equal(off, want)
-    assert np.array_equal(on2, want[: want.size // 2 + 7])
+        for mode in (sg.SEARCH_STREAM, sg.SEARCH_SKIP_ABSENT, sg.SEARCH_EVERY_KMER):
+            ix.set_search_mode(mode)
+            got[mode] = run_reads(ix, letters, rows, cuda, member=True)
+        ix.set_search_mode(sg.SEARCH_STREAM)
+        half = run_reads(ix, letters, rows, cuda, n_kmers=want.size // 2 + 7)
+    nk = want.size
+    bits = np.zeros((nk + 31) // 32 * 32, dtype=bool)
+    bits[:nk] = want != orc.NOT_FOUND
+    words = (bits.reshape(-1, 32).astype(np.uint64) << np.arange(32, dtype=np.uint64)).sum(axis=1).astype(np.uint32)
+    for mode, (ans, mem) in got.items():
+        assert np.array_equal(ans, want), mode
+        assert np.array_equal(mem[: words.size], words), mode
+    assert np.array_equal(half, want[: nk // 2 + 7])
 
 
-def test_absent_run_skip_default_param(cuda):
+def _node_bytes_cpu(seqs, k):
+    """First letter and group-start flag of every node, from the SBWT definition."""
+    keys, dk, dl = orc.independent_sbwt(seqs, k)
+    key = np.concatenate([dk, keys])
+    ln = np.concatenate([dl, np.full(keys.size, k, dtype=np.int64)])
+    order = np.lexsort((ln, key))
+    key, ln = key[order], ln[order]
+    first = np.where(ln >= k, (key & np.uint64(3)).astype(np.int64) + 1, 0)
+    suf = key >> np.uint64(2)  # letters 1..k-1
+    sl = np.minimum(ln, k - 1)
+    start = np.ones(key.size, dtype=bool)
+    start[1:] = (suf[1:] != suf[:-1]) | (sl[1:] != sl[:-1])
+    return (first | (start.astype(np.int64) << 3)).astype(np.uint8)
+
+
+@pytest.mark.parametrize("k", [3, 7, 31, 32])
+def test_node_bytes_match_the_sbwt_definition(cuda, k):
+    rng = wl.rng_for(3100 + k)
+    seqs = [wl.random_bases(rng, 20_000).tobytes(), wl.random_bases(rng, 3_000).tobytes()]
+    built = sg.build_sbwt(seqs, k)
+    want = _node_bytes_cpu(seqs, k)
+    assert want.size == built.n_bits
+    with sg.Index.from_bits(built.bits, built.n_bits, k=k, k_presearch=min(k, 8)) as ix:
+        got = ix.node_bytes()
+    assert np.array_equal(got, want)
+
+
+def test_search_mode_default_param(cuda):
     p = sg.default_params()
-    assert p.skip_absent_runs == 1
+    assert p.search_mode == sg.SEARCH_STREAM
