@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--tpk", type=int, default=0)
     ap.add_argument("--tpb", type=int, default=0)
     ap.add_argument("--layout", choices=["lines", "poppy"], default="lines")
+    ap.add_argument("--sb", type=int, default=1024, help="bits in superblock of the poppy layout")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-e2e", action="store_true")
@@ -255,6 +256,15 @@ def walk_model(ans, steps, rows, k, p, stream, max_rows=20000):
     return searched / max(total, 1), back / max(total, 1)
 
 
+def bits_of(ans):
+    """Membership bitmap of answers: bit j%32 of word j/32 = answer j is not ~0."""
+    import oracle as orc
+    nk = ans.size
+    b = np.zeros((nk + 31) // 32 * 32, dtype=bool)
+    b[:nk] = ans != orc.NOT_FOUND
+    return np.packbits(b.reshape(-1, 32)[:, ::-1], axis=1).view(">u4").reshape(-1).astype(np.uint32)
+
+
 def kernel_traffic(kernel, workload, n_kmers):
     """DRAM bytes of one launch from the committed ncu summary, if it covers this kernel and workload."""
     tp = os.path.join(ROOT, "profiles", "search_kernel_traffic.json")
@@ -309,7 +319,7 @@ def main():
     paths = [f"{prefix}.{c}" for c in "ACGT"]
     layout = sg.SBWT_LAYOUT_POPPY if args.layout == "poppy" else sg.SBWT_LAYOUT_LINES
     t = time.perf_counter()
-    ix = sg.Index.load(*paths, k=k, k_presearch=p, device=local_rank, layout=layout,
+    ix = sg.Index.load(*paths, k=k, k_presearch=p, device=local_rank, layout=layout, bits_in_superblock=args.sb,
                        kmers_per_thread=args.kpt, threads_per_kmer=args.tpk, threads_per_block=args.tpb,
                        search_mode=MODES[args.search_mode])
     runs_form = args.kpt == 0 and args.search_mode != "every" and (args.tpk <= 1 or args.layout == "poppy")
@@ -361,13 +371,14 @@ def main():
     mean_steps = None
     if rank == 0:
         ox = orc.OracleIndex.from_files(paths)
-        table = ox.presearch(p) if p else None
-        rate, ans, steps, nr, threads = cpu_reference(ox, letters, rows, k, p, args.cpu_seconds, table)
+        p_cpu = min(p, 12)  # answers do not depend on p; a CPU table beyond 4^12 entries costs minutes
+        table = ox.presearch(p_cpu) if p_cpu else None
+        rate, ans, steps, nr, threads = cpu_reference(ox, letters, rows, k, p_cpu, args.cpu_seconds, table)
         got = d_ans[: ans.size].cpu().numpy().view(np.uint64)
         if not np.array_equal(got, ans):
             raise SystemExit(f"bench: {int((got != ans).sum())} of {ans.size} sampled answers differ from the oracle")
         mean_steps = float(steps.mean())
-        searched, back = walk_model(ans, steps, rows, k, p, args.search_mode == "stream") if runs_form else (1.0, 0.0)
+        searched, back = walk_model(ans, steps, rows, k, p_cpu, args.search_mode == "stream") if runs_form else (1.0, 0.0)
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"first {nr} reads ({ans.size} k-mers) of the same batch, C restatement of the reference "
                          f"search (the reference has no CPU search), OpenMP schedule(dynamic,4096)"}
@@ -395,6 +406,29 @@ def main():
             raise SystemExit("bench: end-to-end answers differ from the oracle")
         e2e = {"value": n_kmers * world * args.e2e_steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(letters.nbytes + rows.nbytes), "d2h_bytes_per_step": int(n_kmers * 8)}
+        # membership only (sbwt_search_reads_host_member): the bitmap crosses the bus, not the answers
+        n_words = (n_kmers + 31) // 32
+        h_mem = torch.empty(n_words, dtype=torch.int32).pin_memory()
+        ix.member_reads_host(h_letters, h_rows, h_mem)  # warm-up
+        if world > 1:
+            dist.barrier()
+        t = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            ix.member_reads_host(h_letters, h_rows, h_mem)
+        m_s = time.perf_counter() - t
+        if world > 1:
+            tt = torch.tensor([m_s], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            m_s = float(tt.item())
+        if rank == 0:
+            full = ans.size // 32
+            want_bits = bits_of(ans)[:full]
+            if not np.array_equal(h_mem[:full].numpy().view(np.uint32), want_bits):
+                raise SystemExit("bench: end-to-end membership bits differ from the oracle")
+        e2e["membership_only"] = {"value": n_kmers * world * args.e2e_steps / m_s, "unit": UNIT,
+                                  "h2d_bytes_per_step": int(letters.nbytes + rows.nbytes),
+                                  "d2h_bytes_per_step": int(n_words * 4),
+                                  "entry_point": "sbwt_search_reads_host_member"}
 
     # ---- the same batch with every k-mer searched (the reference's per-k-mer work), for comparison
     per_kmer = None
@@ -476,7 +510,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": f"of {peak_kind}",
                          "kernel": kernel, "kernel_ms": kern_ms, "bytes_per_kmer_model": b_kmer,
-                         "mean_steps": mean_steps, "searched_fraction": searched, "backward_step_fraction": back,
+                         "mean_steps": mean_steps, "steps_counted_at_p": p_cpu, "searched_fraction": searched, "backward_step_fraction": back,
                          "dram_frac": (traffic / (kern_ms / 1e3) / 1e9 / peak) if traffic else None,
                          "traffic_source": tr["source"] if tr else None},
             "cpu_baseline": cpu,
@@ -560,6 +594,7 @@ def reference_arm(args, k, p):
     built = sg.build_sbwt([x.tobytes() for x in seqs], k)
     ox = orc.OracleIndex(built.bits, built.n_bits)
     del built
+    p = min(p, 12)  # answers do not depend on p; a CPU table beyond 4^12 entries costs minutes
     table = ox.presearch(p) if p else None
     # each step: a bounded sample of the batch sized to ~budget seconds
     budget = max(1.0, min(args.cpu_seconds, 150.0 / max(args.steps + args.warmup, 1)))

@@ -69,7 +69,7 @@ typedef struct {
  * STREAM: SKIP_ABSENT, and after a k-mer is found the k-mer one letter to its
  *   left is reached by one backward step (a select and a look at the <= 5
  *   nodes of one suffix group) instead of a new search.  Needs the line
- *   layout's index size limit and one byte per column plus select samples,
+ *   layout's index size limit and four bits per column plus select samples,
  *   built on the GPU when the mode is selected. */
 #define SBWT_SEARCH_EVERY_KMER 0
 #define SBWT_SEARCH_SKIP_ABSENT 1
@@ -191,6 +191,7 @@ int sbwt_pack(const uint8_t *d_letters, uint64_t n_letters, uint64_t *d_words, v
  * k-mer, reads in order, to d_answers (device, n_kmers entries, n_kmers =
  * sum of max(0, len-k+1)).  d_member_bits (optional, device, ceil(n_kmers/
  * 32) u32 words) receives bit j%32 of word j/32 = (answer j != -1).
+ * d_answers may be NULL when d_member_bits is given (membership only).
  * Replaces the chain KmerSearch::parse_kmer_string_in_gpu ->
  * create_positions_in_gpu -> call_search (include/epicseq/kmer_search.hpp:
  * 97-185) with one pack kernel and one persistent work-stealing search
@@ -221,6 +222,16 @@ int sbwt_search_reads_noalloc(sbwt_index *index, const uint8_t *d_letters, uint6
  * (results_persister.hpp:58-65). */
 int sbwt_search_reads_host(sbwt_index *index, const uint8_t *letters, uint64_t n_letters, const uint64_t *row_starts,
                            uint64_t n_rows, uint64_t *answers, uint64_t n_kmers);
+
+/* Membership only: as sbwt_search_reads_host, but the result is the bitmap
+ * member_bits (host, ceil(n_kmers/32) u32 words; bit j%32 of word j/32 =
+ * k-mer j is indexed) and no answer array crosses the bus (1 bit instead of
+ * 8 bytes per k-mer).  With the run-walking search modes the kernel writes
+ * only the bitmap.  No reference counterpart (the reference always returns
+ * the colex ranks, results_persister.hpp:58-65). */
+int sbwt_search_reads_host_member(sbwt_index *index, const uint8_t *letters, uint64_t n_letters,
+                                  const uint64_t *row_starts, uint64_t n_rows, uint32_t *member_bits,
+                                  uint64_t n_kmers);
 
 /* Kernel timing of the last sbwt_search_reads call on this index, from CUDA
  * events recorded on that call's stream around each phase (enabled with

@@ -226,6 +226,24 @@ class Index:
         check(lib.sbwt_search_reads_host(self._h, _ptr(letters), int(n_letters), _ptr(rs), n_rows, _ptr(answers), nk))
         return answers[:nk] if isinstance(answers, np.ndarray) else answers
 
+    def member_reads_host(self, letters, row_starts, member_bits=None):
+        """Host reads -> host membership bitmap (uint32 words, bit j%32 of word j/32), streamed
+        through the GPU; only the bitmap crosses the bus."""
+        letters = np.ascontiguousarray(letters, dtype=np.uint8) if isinstance(letters, np.ndarray) else letters
+        rs = row_starts
+        n_rows = (rs.size if isinstance(rs, np.ndarray) else rs.numel()) - 1
+        if isinstance(rs, np.ndarray):
+            rs = np.ascontiguousarray(rs, dtype=np.uint64)
+            nk = int(lib.sbwt_count_kmers(_ptr(rs), n_rows, self.info()["k"]))
+        else:
+            nk = count_kmers(rs.numpy().view(np.uint64), self.info()["k"])
+        if member_bits is None:
+            member_bits = np.empty(max((nk + 31) // 32, 1), dtype=np.uint32)
+        n_letters = letters.size if isinstance(letters, np.ndarray) else letters.numel()
+        check(lib.sbwt_search_reads_host_member(self._h, _ptr(letters), int(n_letters), _ptr(rs), n_rows,
+                                                _ptr(member_bits), nk))
+        return member_bits
+
 
 # ------------------------------------------------------- learned prefilter
 

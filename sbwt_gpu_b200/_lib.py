@@ -127,6 +127,7 @@ SIGNATURES = {
     "sbwt_search_reads_noalloc": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_void_p, c_void_p,
                                           c_uint64, c_void_p]),
     "sbwt_search_reads_host": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_void_p, c_uint64]),
+    "sbwt_search_reads_host_member": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_void_p, c_uint64]),
     "sbwt_count_kmers": (c_uint64, [c_void_p, c_uint64, c_uint32]),
     "sbwt_profile_enable": (c_int, [c_void_p, c_int]),
     "sbwt_use_graphs": (c_int, [c_void_p, c_int]),

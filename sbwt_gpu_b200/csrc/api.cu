@@ -17,8 +17,9 @@ namespace sbwt {
 
 void Workspace::release() {
     cudaFree(words); cudaFree(kstart); cudaFree(chunk_row); cudaFree(scan); cudaFree(counter);
-    cudaFree(letters); cudaFree(rows); cudaFree(answers);
+    cudaFree(letters); cudaFree(rows); cudaFree(answers); cudaFree(member);
     if (h_rows) cudaFreeHost(h_rows);
+    if (h_member) cudaFreeHost(h_member);
     if (h_letters) cudaFreeHost(h_letters);
     if (h_answers) cudaFreeHost(h_answers);
     if (graph) cudaGraphExecDestroy(graph);
@@ -57,6 +58,7 @@ template int grow<unsigned long long>(unsigned long long *&, size_t &, size_t);
 template int grow<uint64_t>(uint64_t *&, size_t &, size_t);
 template int grow_host<uint8_t>(uint8_t *&, size_t &, size_t);
 template int grow_host<uint64_t>(uint64_t *&, size_t &, size_t);
+template int grow_host<uint32_t>(uint32_t *&, size_t &, size_t);
 
 namespace {
 
@@ -410,6 +412,10 @@ int search_rows_device(sbwt_index *ix, Workspace &w, const uint8_t *d_letters, u
     if (n_rows == 0 || n_kmers == 0) return 0;
     const u64 n_words = (n_letters + 32 + 31) / 32;
     SearchArgs a = base_args(ix, true);
+    if (!d_answers && !a.runs) {  // membership only: the per-k-mer kernels derive it from answers
+        SBWT_TRY(grow(w.answers, w.answers_cap, n_kmers));
+        d_answers = w.answers;
+    }
     SBWT_TRY(grow(w.words, w.words_cap, n_words));
     SBWT_TRY(grow(w.kstart, w.kstart_cap, n_rows + 1));
     SBWT_TRY(grow(w.scan, w.scan_cap, scan_scratch_words(n_rows)));
@@ -474,7 +480,7 @@ int enqueue_rows(sbwt_index *ix, Workspace &w, SearchArgs &a, const uint8_t *d_l
     a.chunk_row = w.chunk_row;
     a.n_rows = n_rows;
     a.max_pos = (n_words - 1) * 32 - 1;
-    a.answers = d_answers;
+    a.answers = d_answers;  // NULL (run-walking kernel only): membership bitmap only
     a.n_kmers = n_kmers;
     a.counter = w.counter;
     a.member = a.runs ? d_member : nullptr;  // the run-walking kernel writes the bitmap itself
@@ -528,7 +534,7 @@ extern "C" int sbwt_search_reads(sbwt_index *ix, const uint8_t *d_letters, uint6
     clear_error();
     if (!ix) return set_error("index is NULL");
     if (n_rows && (!d_letters || !d_row_starts)) return set_error("NULL device pointer");
-    if (n_kmers && !d_answers) return set_error("NULL answers pointer");
+    if (n_kmers && !d_answers && !d_member_bits) return set_error("NULL answers and membership pointers");
     SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
     return search_rows_device(ix, ix->ws[0], d_letters, n_letters, d_row_starts, n_rows, d_answers, d_member_bits,
                               n_kmers, (cudaStream_t)stream);

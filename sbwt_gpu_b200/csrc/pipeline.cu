@@ -41,13 +41,16 @@ constexpr u64 kChunkLetters = 64ull << 20;
 
 using namespace sbwt;
 
-extern "C" int sbwt_search_reads_host(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters,
-                                      const uint64_t *row_starts, uint64_t n_rows, uint64_t *answers,
-                                      uint64_t n_kmers) {
-    clear_error();
+namespace sbwt {
+namespace {
+
+// The pipeline behind both host entry points: exactly one of `answers`
+// (u64 per k-mer) and `member` (bit j%32 of word j/32) is non-NULL.
+int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, const uint64_t *row_starts,
+                 uint64_t n_rows, uint64_t *answers, uint32_t *member, uint64_t n_kmers) {
     if (!ix) return set_error("index is NULL");
     if (n_rows == 0) return 0;
-    if (!letters || !row_starts || (n_kmers && !answers)) return set_error("NULL host pointer");
+    if (!letters || !row_starts || (n_kmers && !answers && !member)) return set_error("NULL host pointer");
     if (row_starts[n_rows] > n_letters) return set_error("row_starts[n_rows] exceeds n_letters");
     for (u64 r = 0; r < n_rows; r++)
         if (row_starts[r + 1] < row_starts[r]) return set_error("row_starts must be non-decreasing (row %llu)",
@@ -78,29 +81,54 @@ extern "C" int sbwt_search_reads_host(sbwt_index *ix, const uint8_t *letters, ui
     for (int i = 0; i < 2; i++)
         if (!ix->pipe_stream[i]) SBWT_CHECK_CUDA(cudaStreamCreateWithFlags(&ix->pipe_stream[i], cudaStreamNonBlocking));
     const bool pin_in = is_pinned(letters);
-    const bool pin_out = n_kmers == 0 || is_pinned(answers);
+    const bool pin_out = answers && (n_kmers == 0 || is_pinned(answers));
     u64 max_letters = 0, max_rows = 0, max_k = 0;
     for (const Chunk &c : chunks) {
         max_letters = std::max(max_letters, c.l1 - c.l0);
         max_rows = std::max(max_rows, c.r1 - c.r0);
         max_k = std::max(max_k, c.nk);
     }
+    const u64 max_words = (max_k + 31) / 32;
     for (int i = 0; i < 2; i++) {
         Workspace &w = ix->ws[i];
         SBWT_TRY(grow(w.letters, w.letters_cap, max_letters + 16));
         SBWT_TRY(grow(w.rows, w.rows_cap, max_rows + 1));
-        SBWT_TRY(grow(w.answers, w.answers_cap, max_k));
         SBWT_TRY(grow_host(w.h_rows, w.h_rows_cap, max_rows + 1));
         if (!pin_in) SBWT_TRY(grow_host(w.h_letters, w.h_letters_cap, max_letters + 16));
-        if (!pin_out) SBWT_TRY(grow_host(w.h_answers, w.h_answers_cap, max_k));
+        if (answers) {
+            SBWT_TRY(grow(w.answers, w.answers_cap, max_k));
+            if (!pin_out) SBWT_TRY(grow_host(w.h_answers, w.h_answers_cap, max_k));
+        } else {
+            SBWT_TRY(grow(w.member, w.member_cap, max_words + 1));
+            SBWT_TRY(grow_host(w.h_member, w.h_member_cap, max_words + 1));
+        }
     }
-    // pending[i]: chunk whose answers sit in slot i's pinned staging (pageable output)
+    if (member) std::memset(member, 0, (n_kmers + 31) / 32 * sizeof(uint32_t));
+    // pending[i]: chunk whose results sit in slot i's pinned staging
     long pending[2] = {-1, -1};
     auto drain = [&](int slot) -> int {
         SBWT_CHECK_CUDA(cudaStreamSynchronize(ix->pipe_stream[slot]));
         if (pending[slot] >= 0) {
             const Chunk &c = chunks[(size_t)pending[slot]];
-            std::memcpy(answers + c.k0, ix->ws[slot].h_answers, c.nk * sizeof(u64));
+            if (answers) {
+                std::memcpy(answers + c.k0, ix->ws[slot].h_answers, c.nk * sizeof(u64));
+            } else {
+                // the chunk's bitmap starts at bit k0 of the output: shift it into place
+                const uint32_t *src = ix->ws[slot].h_member;
+                const u64 nw = (c.nk + 31) / 32, w0 = c.k0 >> 5;
+                const u32 sh = (u32)(c.k0 & 31u);
+                const u64 out_words = (n_kmers + 31) / 32;
+                if (sh == 0) {
+                    for (u64 i = 0; i < nw; i++) member[w0 + i] |= src[i];
+                } else {
+                    // word w0+i gets the high part of src[i-1] and the low part of src[i]
+                    uint32_t *dst = member + w0;
+                    dst[0] |= src[0] << sh;
+#pragma omp parallel for schedule(static) if (nw > (1u << 16))
+                    for (int64_t i = 1; i < (int64_t)nw; i++) dst[i] |= (src[i] << sh) | (src[i - 1] >> (32u - sh));
+                    if (w0 + nw < out_words) dst[nw] |= src[nw - 1] >> (32u - sh);
+                }
+            }
             pending[slot] = -1;
         }
         return 0;
@@ -120,17 +148,45 @@ extern "C" int sbwt_search_reads_host(sbwt_index *ix, const uint8_t *letters, ui
             std::memcpy(w.h_letters, letters + c.l0, nl);
             SBWT_CHECK_CUDA(cudaMemcpyAsync(w.letters, w.h_letters, nl, cudaMemcpyHostToDevice, s));
         }
-        SBWT_TRY(search_rows_device(ix, w, w.letters, nl, w.rows, nr, w.answers, nullptr, c.nk, s));
-        if (c.nk) {
-            if (pin_out) {
-                SBWT_CHECK_CUDA(cudaMemcpyAsync(answers + c.k0, w.answers, c.nk * sizeof(u64), cudaMemcpyDeviceToHost, s));
-            } else {
-                SBWT_CHECK_CUDA(cudaMemcpyAsync(w.h_answers, w.answers, c.nk * sizeof(u64), cudaMemcpyDeviceToHost, s));
-                pending[slot] = (long)b;
+        if (answers) {
+            SBWT_TRY(search_rows_device(ix, w, w.letters, nl, w.rows, nr, w.answers, nullptr, c.nk, s));
+            if (c.nk) {
+                if (pin_out) {
+                    SBWT_CHECK_CUDA(cudaMemcpyAsync(answers + c.k0, w.answers, c.nk * sizeof(u64),
+                                                    cudaMemcpyDeviceToHost, s));
+                } else {
+                    SBWT_CHECK_CUDA(cudaMemcpyAsync(w.h_answers, w.answers, c.nk * sizeof(u64),
+                                                    cudaMemcpyDeviceToHost, s));
+                    pending[slot] = (long)b;
+                }
             }
+        } else if (c.nk) {
+            SBWT_TRY(search_rows_device(ix, w, w.letters, nl, w.rows, nr, nullptr, w.member, c.nk, s));
+            SBWT_CHECK_CUDA(cudaMemcpyAsync(w.h_member, w.member, (c.nk + 31) / 32 * sizeof(uint32_t),
+                                            cudaMemcpyDeviceToHost, s));
+            pending[slot] = (long)b;
         }
     }
     SBWT_TRY(drain(0));
     SBWT_TRY(drain(1));
     return 0;
+}
+
+}  // namespace
+}  // namespace sbwt
+
+extern "C" int sbwt_search_reads_host(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters,
+                                      const uint64_t *row_starts, uint64_t n_rows, uint64_t *answers,
+                                      uint64_t n_kmers) {
+    clear_error();
+    if (n_kmers && !answers) return set_error("NULL host pointer");
+    return run_pipeline(ix, letters, n_letters, row_starts, n_rows, answers, nullptr, n_kmers);
+}
+
+extern "C" int sbwt_search_reads_host_member(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters,
+                                             const uint64_t *row_starts, uint64_t n_rows, uint32_t *member_bits,
+                                             uint64_t n_kmers) {
+    clear_error();
+    if (n_kmers && !member_bits) return set_error("NULL host pointer");
+    return run_pipeline(ix, letters, n_letters, row_starts, n_rows, nullptr, member_bits, n_kmers);
 }

@@ -12,6 +12,7 @@
 // Then first letter = letter k-1 (or $ if len < k), and v starts a group iff
 // its last k-1 letters (and how many of them are real) differ from v-1's.
 #include <cstring>
+#include <vector>
 
 #include "internal.h"
 #include "stream.cuh"
@@ -73,20 +74,27 @@ __global__ void double_kernel(u32 n, u32 m, const u32 *__restrict__ P, const u64
     P2[v] = P[u];
 }
 
-__global__ void node_bytes_kernel(u32 n, u32 k, const u64 *__restrict__ code, const uint8_t *__restrict__ len,
-                                  uint8_t *__restrict__ node) {
-    const u32 v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    const u64 mask = (k - 1u >= 32u) ? ~0ull : ((1ull << (2u * (k - 1u))) - 1ull);
-    const u32 l = len[v];
-    const u64 c = code[v];
-    const u32 first = l >= k ? (u32)((c >> (2u * (k - 1u))) & 3u) + 1u : 0u;
-    bool start = v == 0;
-    if (!start) {
-        const u32 lp = len[v - 1];
-        start = ((c ^ code[v - 1]) & mask) != 0 || min(l, k - 1u) != min(lp, k - 1u);
+// One thread per byte: the nibbles of nodes 2t and 2t+1.
+__global__ void node_nibbles_kernel(u32 n, u32 k, const u64 *__restrict__ code, const uint8_t *__restrict__ len,
+                                   uint8_t *__restrict__ node) {
+    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((u64)t * 2u >= n) return;
+    const u64 mask = (1ull << (2u * (k - 1u))) - 1ull;  // the last k-1 letters (k <= 32)
+    u32 byte = 0;
+    for (u32 h = 0; h < 2u; h++) {
+        const u32 v = 2u * t + h;
+        if (v >= n) break;
+        const u32 l = len[v];
+        const u64 c = code[v];
+        const u32 first = l >= k ? (u32)((c >> (2u * (k - 1u))) & 3u) + 1u : 0u;
+        bool start = v == 0;
+        if (!start) {
+            const u32 lp = len[v - 1];
+            start = ((c ^ code[v - 1]) & mask) != 0 || min(l, k - 1u) != min(lp, k - 1u);
+        }
+        byte |= (first | (start ? kGroupStart : 0u)) << (4u * h);
     }
-    node[v] = (uint8_t)(first | (start ? kGroupStart : 0u));
+    node[t] = (uint8_t)byte;
 }
 
 }  // namespace
@@ -121,7 +129,7 @@ int build_stream(sbwt_index *ix, cudaStream_t s) {
     }
     SBWT_CHECK_CUDA(cudaMalloc(&ix->d_sel, total * sizeof(u32)));
     SBWT_CHECK_CUDA(cudaMemsetAsync(ix->d_sel, 0, total * sizeof(u32), s));
-    SBWT_CHECK_CUDA(cudaMalloc(&ix->d_node, (size_t)n + 16));
+    SBWT_CHECK_CUDA(cudaMalloc(&ix->d_node, (size_t)n / 2 + 16));
     for (int c = 0; c < 4; c++) {
         if (!ix->sel_n[c]) continue;
         select_samples_kernel<<<(ix->lpc + 255) / 256, 256, 0, s>>>(ix->d_lines + (u64)c * ix->lpc, ix->lpc,
@@ -158,7 +166,7 @@ int build_stream(sbwt_index *ix, cudaStream_t s) {
                                                  len[cur ^ 1]);
             cur ^= 1;
         }
-        node_bytes_kernel<<<blocks, 256, 0, s>>>(n, ix->k, code[cur], len[cur], ix->d_node);
+        node_nibbles_kernel<<<(n / 2 + 1 + 255) / 256, 256, 0, s>>>(n, ix->k, code[cur], len[cur], ix->d_node);
         unsigned long long h_bad = 0;
         e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaMemcpyAsync(&h_bad, bad, sizeof h_bad, cudaMemcpyDeviceToHost, s);
@@ -194,6 +202,8 @@ extern "C" int sbwt_node_bytes_export(sbwt_index *ix, uint8_t *out, uint64_t cou
     if (count != ix->n) return set_error("count must be the number of columns (%llu)", (unsigned long long)ix->n);
     SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
     SBWT_TRY(build_stream(ix, 0));
-    SBWT_CHECK_CUDA(cudaMemcpy(out, ix->d_node, count, cudaMemcpyDeviceToHost));
+    std::vector<uint8_t> packed(count / 2 + 1);
+    SBWT_CHECK_CUDA(cudaMemcpy(packed.data(), ix->d_node, count / 2 + (count & 1), cudaMemcpyDeviceToHost));
+    for (u64 v = 0; v < count; v++) out[v] = (uint8_t)((packed[v >> 1] >> ((v & 1) * 4)) & 15u);
     return 0;
 }

@@ -11,8 +11,9 @@
 // So from the node v of the k-mer y.b, the node of the k-mer a.y (one letter
 // to the left in the read) is the member of the group starting at
 // select_b(v - C[b]) whose first letter is a, if there is one.  Per node the
-// engine keeps one byte: its first letter (0 = $, 1..4 = A..T) and a flag for
-// the first node of its group (bit 3).  select_c uses the line counts plus a
+// engine keeps four bits, two nodes per byte (even node in the low half): its
+// first letter (0 = $, 1..4 = A..T) and a flag for the first node of its
+// group (bit 3).  select_c uses the line counts plus a
 // sample of the line holding every 64th one.
 #pragma once
 #include "device.cuh"
@@ -21,7 +22,7 @@ namespace sbwt {
 namespace dev {
 
 constexpr u32 kSelLog = 6;          // one select sample per 64 ones
-constexpr uint8_t kGroupStart = 8;  // node byte: bit 3 = first node of its group
+constexpr uint8_t kGroupStart = 8;  // node nibble: bit 3 = first node of its group
 constexpr u32 kNoNode = 0;          // node 0 (the all-$ root) is never a k-mer's node
 
 // Position of the (i+1)-th one (0-based i) of the 64-bit MSB-first word w.
@@ -46,8 +47,8 @@ __device__ __forceinline__ u32 line_select(const ulonglong4 *__restrict__ lines,
                                            u32 n_samples, u32 i) {
     const u32 s = i >> kSelLog;
     if (s >= n_samples) return ~0u;
-    u32 lo = __ldg(sel + s);
-    u32 hi = s + 1 < n_samples ? __ldg(sel + s + 1) : lpc - 1;
+    u32 lo = ld_keep_u32(sel + s);
+    u32 hi = s + 1 < n_samples ? ld_keep_u32(sel + s + 1) : lpc - 1;
     // last line in [lo, hi] whose count is <= i (its count word is the line's first 8 bytes)
     while (lo < hi) {
         const u32 mid = (lo + hi + 1) >> 1;
@@ -80,7 +81,7 @@ struct StreamView {
     const u32 *sel;        // 4 sample arrays, vector c at sel + sel_off[c]
     u32 sel_off[4];
     u32 sel_n[4];
-    const uint8_t *node;   // per node: first letter | kGroupStart
+    const uint8_t *node;   // per node a nibble (first letter | kGroupStart), two per byte
     u32 n;                 // nodes
     u32 C[4];
 
@@ -102,7 +103,7 @@ struct StreamView {
         const u32 want = a + 1u;
 #pragma unroll 1
         for (u32 g = 0; g < 5u && u < n; g++, u++) {
-            const u32 f = __ldg(node + u);
+            const u32 f = (ld_keep_u8(node + (u >> 1)) >> ((u & 1u) << 2)) & 15u;
             if (g && (f & kGroupStart)) break;
             const u32 first = f & 7u;
             if (first == want) return u;

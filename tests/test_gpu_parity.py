@@ -427,3 +427,58 @@ def test_node_bytes_match_the_sbwt_definition(cuda, k):
 def test_search_mode_default_param(cuda):
     p = sg.default_params()
     assert p.search_mode == sg.SEARCH_STREAM
+
+
+def _bits_of(ans):
+    nk = ans.size
+    b = np.zeros((nk + 31) // 32 * 32, dtype=bool)
+    b[:nk] = ans != orc.NOT_FOUND
+    return (b.reshape(-1, 32).astype(np.uint64) << np.arange(32, dtype=np.uint64)).sum(axis=1).astype(np.uint32)
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_membership_only_device_and_host(small, cuda, mode):
+    """Answers NULL + bitmap (device entry point) and the host membership pipeline, every mode,
+    with chunks whose first k-mer is not a multiple of 32."""
+    import torch
+    b, k = small["built"], small["k"]
+    rng = np.random.default_rng(5)
+    lens = rng.integers(20, 400, size=3000)
+    g = small["genome"]
+    parts = [g[s:s + n] if i % 3 else wl.random_bases(rng, int(n)) for i, (s, n) in
+             enumerate(zip(rng.integers(0, g.size - 400, size=lens.size), lens))]
+    letters = np.concatenate(parts)
+    rows = np.zeros(len(parts) + 1, dtype=np.uint64)
+    rows[1:] = np.cumsum([p.size for p in parts])
+    ox = orc.OracleIndex(b.bits, b.n_bits)
+    want = _bits_of(ox.search_reads(letters, rows, k, 10))
+    with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=10, search_mode=mode) as ix:
+        nk = sg.count_kmers(rows, k)
+        d_mem = torch.full(((nk + 31) // 32,), -1, dtype=torch.int32, device=cuda)
+        ix.search_reads(_t(letters, cuda), _t(rows, cuda), None, nk, d_member_bits=d_mem)
+        torch.cuda.synchronize()
+        got_dev = d_mem.cpu().numpy().view(np.uint32)
+        got_host = ix.member_reads_host(letters, rows)
+    assert np.array_equal(got_dev, want)
+    assert np.array_equal(got_host[: want.size], want)
+
+
+def test_host_pipelines_across_chunks(small, cuda):
+    """More than one 64M-letter chunk: the answers pipeline and the membership pipeline (whose
+    second chunk starts at a k-mer index that is not a multiple of 32) against one device search."""
+    import torch
+    b, k = small["built"], small["k"]
+    rng = wl.rng_for(77)
+    g = small["genome"]
+    n_reads = 470_000
+    reads = np.concatenate([wl.sampled_reads(rng, g, n_reads // 10, 150, 0.01),
+                            wl.uniform_reads(rng, n_reads - n_reads // 10, 150)])
+    letters = np.ascontiguousarray(reads).reshape(-1)
+    rows = np.arange(n_reads + 1, dtype=np.uint64) * np.uint64(150)
+    with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=10) as ix:
+        want = run_reads(ix, letters, rows, cuda)
+        host = ix.search_reads_host(letters, rows)
+        mem = ix.member_reads_host(letters, rows)
+    assert letters.size > (64 << 20)
+    assert np.array_equal(host, want)
+    assert np.array_equal(mem, _bits_of(want))
