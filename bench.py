@@ -25,6 +25,7 @@ the reference has no CPU search, so its arm is the C restatement in oracle/
 import argparse
 import json
 import os
+import shutil
 import statistics
 import subprocess
 import sys
@@ -102,6 +103,7 @@ def workload_of(args, rank):
             wl.write_fasta(path, lt, rw)
             paths.append(path)
         letters, rows, _, _ = sg.read_queries_many(paths, 31)
+        shutil.rmtree(d, ignore_errors=True)
         return [genome], letters, rows, 10
     # pangenome
     rng = wl.rng_for(1239)
@@ -256,6 +258,17 @@ def walk_model(ans, steps, rows, k, p, stream, max_rows=20000):
     return searched / max(total, 1), back / max(total, 1)
 
 
+def max_over_ranks(x):
+    """Max of a per-rank number over all ranks of the process group (device tensor under NCCL,
+    host tensor under gloo)."""
+    import torch
+    import torch.distributed as dist
+    dev = torch.device("cpu") if dist.get_backend() == "gloo" else torch.device("cuda", torch.cuda.current_device())
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def bits_of(ans):
     """Membership bitmap of answers: bit j%32 of word j/32 = answer j is not ~0."""
     import oracle as orc
@@ -361,9 +374,7 @@ def main():
     clk = clocks.stop()
     if world > 1:
         dist.barrier()
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+        total_ms = max_over_ranks(total_ms)
     value = n_kmers * world * args.steps / (total_ms / 1e3)
 
     # ---- correctness on a sample + the CPU baseline (rank 0 only, untimed)
@@ -399,9 +410,7 @@ def main():
             ix.search_reads_host(h_letters, h_rows, h_ans)
         e2e_s = time.perf_counter() - t
         if world > 1:
-            tt = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_s = float(tt.item())
+            e2e_s = max_over_ranks(e2e_s)
         if rank == 0 and not np.array_equal(h_ans[: ans.size].numpy().view(np.uint64), ans):
             raise SystemExit("bench: end-to-end answers differ from the oracle")
         e2e = {"value": n_kmers * world * args.e2e_steps / e2e_s, "unit": UNIT,
@@ -417,9 +426,7 @@ def main():
             ix.member_reads_host(h_letters, h_rows, h_mem)
         m_s = time.perf_counter() - t
         if world > 1:
-            tt = torch.tensor([m_s], dtype=torch.float64, device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            m_s = float(tt.item())
+            m_s = max_over_ranks(m_s)
         if rank == 0:
             full = ans.size // 32
             want_bits = bits_of(ans)[:full]
