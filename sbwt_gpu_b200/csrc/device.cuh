@@ -32,109 +32,25 @@ constexpr u32 kLineBits = 224;      // data bits per 32-byte line
 constexpr u32 kLineBytes = 32;
 constexpr u32 kMaxLinesPerChar = 1u << 24;  // 32-bit counts: 224 * 2^24 < 2^32
 
-// L2 residency hints (build option SBWT_L2_HINTS=1): index data (lines, rank
-// words, bit blocks, node nibbles, select samples) is loaded with an
-// evict_last policy, streamed data (presearch entries, packed letters,
-// answers) with evict_first, so that the gathers of the search keep the index
-// in L2.  createpolicy and the .L2::cache_hint forms are PTX ISA 7.4+, sm_80+.
-#ifndef SBWT_L2_HINTS
-#define SBWT_L2_HINTS 0
-#endif
-
-__device__ __forceinline__ u64 l2_keep() {
-    u64 p;
-    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
-
-__device__ __forceinline__ u64 l2_stream() {
-    u64 p;
-    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
-
 // 256-bit read-only load of one line (sm_100 supports .v4.u64 global loads).
 __device__ __forceinline__ ulonglong4 ld_line(const ulonglong4 *p) {
     ulonglong4 v;
-#if SBWT_L2_HINTS
-    asm("ld.global.nc.L2::cache_hint.v4.u64 {%0, %1, %2, %3}, [%4], %5;"
-        : "=l"(v.x), "=l"(v.y), "=l"(v.z), "=l"(v.w)
-        : "l"(p), "l"(l2_keep()));
-#else
     asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];"
         : "=l"(v.x), "=l"(v.y), "=l"(v.z), "=l"(v.w)
         : "l"(p));
-#endif
     return v;
 }
 
 __device__ __forceinline__ ulonglong2 ld_nc2(const ulonglong2 *p) {
     ulonglong2 v;
-#if SBWT_L2_HINTS
-    asm("ld.global.nc.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;" : "=l"(v.x), "=l"(v.y) : "l"(p), "l"(l2_keep()));
-#else
     asm("ld.global.nc.v2.u64 {%0, %1}, [%2];" : "=l"(v.x), "=l"(v.y) : "l"(p));
-#endif
     return v;
 }
 
 __device__ __forceinline__ u64 ld_nc(const u64 *p) {
     u64 v;
-#if SBWT_L2_HINTS
-    asm("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(p), "l"(l2_keep()));
-#else
     asm("ld.global.nc.u64 %0, [%1];" : "=l"(v) : "l"(p));
-#endif
     return v;
-}
-
-__device__ __forceinline__ u32 ld_keep_u32(const u32 *p) {
-    u32 v;
-#if SBWT_L2_HINTS
-    asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(l2_keep()));
-#else
-    asm("ld.global.nc.u32 %0, [%1];" : "=r"(v) : "l"(p));
-#endif
-    return v;
-}
-
-__device__ __forceinline__ u32 ld_keep_u8(const uint8_t *p) {
-    u32 v;
-#if SBWT_L2_HINTS
-    asm("ld.global.nc.L2::cache_hint.u8 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(l2_keep()));
-#else
-    asm("ld.global.nc.u8 %0, [%1];" : "=r"(v) : "l"(p));
-#endif
-    return v;
-}
-
-// Streamed data: a presearch entry {l, r}, a word of packed letters, an answer.
-__device__ __forceinline__ uint2 ld_stream_pair(const uint2 *p) {
-    uint2 v;
-#if SBWT_L2_HINTS
-    asm("ld.global.nc.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;" : "=r"(v.x), "=r"(v.y) : "l"(p), "l"(l2_stream()));
-#else
-    asm("ld.global.nc.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
-#endif
-    return v;
-}
-
-__device__ __forceinline__ u64 ld_stream_u64(const u64 *p) {
-    u64 v;
-#if SBWT_L2_HINTS
-    asm("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(p), "l"(l2_stream()));
-#else
-    asm("ld.global.nc.u64 %0, [%1];" : "=l"(v) : "l"(p));
-#endif
-    return v;
-}
-
-__device__ __forceinline__ void st_stream_u64(u64 *p, u64 v) {
-#if SBWT_L2_HINTS
-    asm volatile("st.global.L2::cache_hint.u64 [%0], %1, %2;" ::"l"(p), "l"(v), "l"(l2_stream()) : "memory");
-#else
-    asm volatile("st.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-#endif
 }
 
 // x >> s with the PTX rule that s >= 64 gives 0 (the reference relies on it,

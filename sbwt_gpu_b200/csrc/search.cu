@@ -357,11 +357,16 @@ __global__ void __launch_bounds__(128) search_queue_kernel(const R rk, const Sea
 
 constexpr u32 kWin = 32;            // k-mers per window (granularity of chunk_row)
 
-// Resident-block floor of the run-walking kernel (build option; 1 lets the
-// compiler pick the register count).
-#ifndef SBWT_RUNS_MIN_BLOCKS
-#define SBWT_RUNS_MIN_BLOCKS 1
-#endif
+// Resident 128-thread blocks per SM the run-walking kernel is compiled for
+// (a register cap), measured on the large workload: 9 for the line ranker
+// (56 registers; 8 blocks at the compiler's 60 registers was 13 % slower),
+// 10 for the poppy ranker with basic blocks of up to 256 bits (48 registers);
+// the larger poppy blocks keep the compiler's choice (a cap spills there).
+template <class R> struct RunsMinBlocks { static constexpr int value = 1; };
+template <int TPK> struct RunsMinBlocks<LinesRankerT<TPK>> { static constexpr int value = 9; };
+template <int SB, int KIND, class IT, int TPK> struct RunsMinBlocks<PoppyRanker<SB, KIND, IT, TPK>> {
+    static constexpr int value = SB <= 1024 ? 10 : 1;
+};
 constexpr u32 kStart = 0xfffffffeu; // lane state: start the run's current k-mer
 
 struct RunEntry {
@@ -371,7 +376,7 @@ struct RunEntry {
 };
 
 template <class R, bool STREAM>
-__global__ void __launch_bounds__(128, SBWT_RUNS_MIN_BLOCKS) search_runs_kernel(const R rk, const SearchArgs a) {
+__global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kernel(const R rk, const SearchArgs a) {
     static_assert(sizeof(typename R::IT) == 4, "the run form serves 32-bit intervals");
     __shared__ RunEntry queue[kQueueWarps][kQueue];
     using PT = uint2;
@@ -405,7 +410,7 @@ __global__ void __launch_bounds__(128, SBWT_RUNS_MIN_BLOCKS) search_runs_kernel(
                 } else {
                     const u64 end = min((u64)base + 32u * kWin, n_eff);
                     if (a.answers)  // NULL: membership bitmap only
-                        for (u64 t = base + lane; t < end; t += 32u) st_stream_u64(a.answers + t, ~0ull);
+                        for (u64 t = base + lane; t < end; t += 32u) a.answers[t] = ~0ull;
                     pj = min((u64)base + (u64)lane * kWin, end);
                     pe = min(pj + kWin, end);
                     if (pj < pe) {
@@ -454,18 +459,18 @@ __global__ void __launch_bounds__(128, SBWT_RUNS_MIN_BLOCKS) search_runs_kernel(
         if (I == kStart) {
             if (STREAM && V != dev::kNoNode) {
                 // ---- backward step: k-mer J = x[J] . (first k-1 letters of k-mer J+1)
-                const u32 letter = (u32)(ld_stream_u64(a.words + (pos >> 5)) >> (62u - 2u * (u32)(pos & 31u))) & 3u;
+                const u32 letter = (u32)(a.words[pos >> 5] >> (62u - 2u * (u32)(pos & 31u))) & 3u;
                 const u32 u = a.sv.back_step(V, letter);
                 adv = 1;
                 if (u != dev::kNoNode) found = u;
             } else {
                 // ---- start: letters (search_kernel.hpp:66-68) and presearch entry (:71-82)
                 const u64 b = min(pos, a.max_pos) << 1;
-                const u64 w0 = ld_stream_u64(a.words + (b >> 6)), w1 = ld_stream_u64(a.words + (b >> 6) + 1);
+                const u64 w0 = a.words[b >> 6], w1 = a.words[(b >> 6) + 1];
                 const u32 sh = (u32)(b & 63u);
                 kmer = (w0 << sh) | (shr_clamp(w1, 63u - sh) >> 1);
                 if (p) {
-                    const PT e = ld_stream_pair(pre + (kmer >> (64u - 2u * p)));
+                    const PT e = pre[kmer >> (64u - 2u * p)];
                     L = e.x;
                     Rr = e.y;
                 } else {
@@ -497,7 +502,7 @@ __global__ void __launch_bounds__(128, SBWT_RUNS_MIN_BLOCKS) search_runs_kernel(
             }
         }
         if (found != ~0u) {
-            if (a.answers) st_stream_u64(a.answers + J, (u64)found);
+            if (a.answers) a.answers[J] = (u64)found;
             if (member) atomicOr(member + (J >> 5), 1u << (J & 31u));
         }
         if (adv) {

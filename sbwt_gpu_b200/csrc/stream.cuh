@@ -47,8 +47,8 @@ __device__ __forceinline__ u32 line_select(const ulonglong4 *__restrict__ lines,
                                            u32 n_samples, u32 i) {
     const u32 s = i >> kSelLog;
     if (s >= n_samples) return ~0u;
-    u32 lo = ld_keep_u32(sel + s);
-    u32 hi = s + 1 < n_samples ? ld_keep_u32(sel + s + 1) : lpc - 1;
+    u32 lo = __ldg(sel + s);
+    u32 hi = s + 1 < n_samples ? __ldg(sel + s + 1) : lpc - 1;
     // last line in [lo, hi] whose count is <= i (its count word is the line's first 8 bytes)
     while (lo < hi) {
         const u32 mid = (lo + hi + 1) >> 1;
@@ -103,7 +103,7 @@ struct StreamView {
         const u32 want = a + 1u;
 #pragma unroll 1
         for (u32 g = 0; g < 5u && u < n; g++, u++) {
-            const u32 f = (ld_keep_u8(node + (u >> 1)) >> ((u & 1u) << 2)) & 15u;
+            const u32 f = (u32)(__ldg(node + (u >> 1)) >> ((u & 1u) << 2)) & 15u;
             if (g && (f & kGroupStart)) break;
             const u32 first = f & 7u;
             if (first == want) return u;

@@ -123,3 +123,40 @@ def test_prefilter_logits_api(trained, cuda):
     torch.cuda.synchronize()
     want, _ = mo.forward(theta, kmers, k)
     assert np.allclose(d_l.cpu().numpy(), want, rtol=2e-2, atol=2e-2)
+
+
+def _auc(pos, neg):
+    """Probability that a positive's logit exceeds a negative's (ties count half)."""
+    allv = np.concatenate([pos, neg])
+    ranks = np.argsort(np.argsort(allv, kind="mergesort"), kind="mergesort").astype(np.float64) + 1
+    return (ranks[: pos.size].sum() - pos.size * (pos.size + 1) / 2) / (pos.size * neg.size)
+
+
+def test_trained_network_gains_over_the_untrained_one(trained, cuda):
+    """What training buys, at the same threshold and Bloom settings: the trained network
+    separates indexed k-mers from random ones (AUC) and sends fewer indexed k-mers to the backup
+    Bloom filter (a smaller filter for the same false-positive rate); both sandwiches stay exact."""
+    import torch
+    ix, pf, k = trained["ix"], trained["pf"], trained["k"]
+    with sg.Prefilter.train(ix, steps=1, batch=2048, n_positive=400_000, n_negative=400_000, seed=9) as base:
+        g = trained["genome"]
+        pos = orc.extract_kmers(g, np.array([0, g.size], dtype=np.uint64), k)[:20_000]
+        neg = _rand_kmers(np.random.default_rng(8), 20_000, k)
+        out = {}
+        for name, f in (("trained", pf), ("untrained", base)):
+            d = torch.from_numpy(np.concatenate([pos, neg]).view(np.int64)).to(cuda)
+            lg = torch.empty(d.numel(), dtype=torch.float32, device=cuda)
+            f.logits(d, lg)
+            torch.cuda.synchronize()
+            lg = lg.cpu().numpy()
+            rng = wl.rng_for(5)
+            letters, rows = wl.kmer_queries(rng, g, 20_000, k, neg_frac=0.9)
+            qk = torch.from_numpy(orc.extract_kmers(letters, rows, k).view(np.int64)).to(cuda)
+            ans = torch.empty_like(qk)
+            skipped = ix.search_kmers_filtered(f, qk, ans)
+            out[name] = {"auc": _auc(lg[: pos.size], lg[pos.size:]), "skip": skipped / qk.numel(),
+                         "rejected_indexed": f.stats()["n_rejected_indexed"]}
+    t, u = out["trained"], out["untrained"]
+    assert t["auc"] > 0.9 and t["auc"] > u["auc"] + 0.2, out
+    assert t["rejected_indexed"] < 0.8 * u["rejected_indexed"], out
+    assert t["skip"] > 0 and u["skip"] > 0, out
