@@ -4,7 +4,12 @@ the kernel time the reference itself prints ("Search in GPU: X ms",
 include/epicseq/kmer_search.hpp:167-169; CUDA events around the kernel,
 include/gpu/search_and_presearch_launchers.hpp:41,53-54).
 
-    python tests/golden/reference_gpu_timing.py [--scale S] [--out FILE]
+    python tests/golden/reference_gpu_timing.py [--scale S] [--out FILE] [--cli]
+
+With --cli both programs also store their answers (the reference's stdout
+format) and the wall time of each whole program run is recorded: the
+reference's build/search against this project's sbwt_search, same flags,
+same index files and query file; the two outputs must be byte-identical.
 
 The inputs satisfy the reference's in-bounds conditions (make_golden.check_safe):
 150 bp ACGT reads, a k-mer count that is a multiple of 64 with
@@ -29,6 +34,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--cli", action="store_true", help="also time both programs end to end with stored results")
     args = ap.parse_args()
     import bench
     import make_golden
@@ -65,11 +71,40 @@ def main():
         "flags": " ".join(f for f in flags if not f.startswith("--file")),
     }
     res["search_kmers_per_s"] = n_kmers / (res["search_ms"] / 1e3) if res["search_ms"] else None
+    if args.cli:
+        res["cli"] = time_programs(d, flags, env)
     line = json.dumps(res)
     print(line)
     if args.out:
         with open(args.out, "w") as f:
             f.write(line + "\n")
+
+
+def time_programs(d, flags, env):
+    """Wall time of each program writing its answers to a file, and the outputs' SHA-256."""
+    import hashlib
+    import time
+    import sbwt_gpu_b200 as sg
+    import make_golden
+    store = [f for f in flags if f != "--do-not-store-results"]
+    out = {}
+    for name, exe in (("reference", make_golden.REF_SEARCH), ("ours", sg.CLI_PATH)):
+        path = os.path.join(d, f"{name}.out")
+        with open(path, "wb") as f:
+            t = time.perf_counter()
+            r = subprocess.run([exe] + store, stdout=f, stderr=subprocess.PIPE, env=env, timeout=3600)
+            wall = time.perf_counter() - t
+        if r.returncode != 0 or (name == "reference" and make_golden.reference_failed(r.stderr)):
+            raise SystemExit(f"{name} failed: {r.stderr.decode(errors='replace')[-2000:]}")
+        h = hashlib.sha256()
+        with open(path, "rb") as f:
+            for block in iter(lambda: f.read(1 << 24), b""):
+                h.update(block)
+        out[name] = {"wall_s": wall, "bytes": os.path.getsize(path), "sha256": h.hexdigest(),
+                     "stderr_tail": r.stderr.decode(errors="replace")[-600:]}
+        os.remove(path)
+    out["identical"] = out["reference"]["sha256"] == out["ours"]["sha256"]
+    return out
 
 
 if __name__ == "__main__":
