@@ -133,12 +133,13 @@ def _auc(pos, neg):
 
 
 def test_trained_network_gains_over_the_untrained_one(trained, cuda):
-    """What training buys, at the same threshold and Bloom settings: the trained network
-    separates indexed k-mers from random ones (AUC) and sends fewer indexed k-mers to the backup
-    Bloom filter (a smaller filter for the same false-positive rate); both sandwiches stay exact."""
+    """What training buys over the same sandwich with the untrained (initial) network, at the
+    same threshold and Bloom settings: the trained network separates indexed k-mers from random
+    ones (AUC), sends far fewer indexed k-mers to the backup Bloom filter (a smaller filter for
+    the same false-positive rate) and skips more of a 90%-negative query set."""
     import torch
     ix, pf, k = trained["ix"], trained["pf"], trained["k"]
-    with sg.Prefilter.train(ix, steps=1, batch=2048, n_positive=400_000, n_negative=400_000, seed=9) as base:
+    with sg.Prefilter.train(ix, steps=0, batch=2048, n_positive=400_000, n_negative=400_000, seed=9) as base:
         g = trained["genome"]
         pos = orc.extract_kmers(g, np.array([0, g.size], dtype=np.uint64), k)[:20_000]
         neg = _rand_kmers(np.random.default_rng(8), 20_000, k)
@@ -157,6 +158,6 @@ def test_trained_network_gains_over_the_untrained_one(trained, cuda):
             out[name] = {"auc": _auc(lg[: pos.size], lg[pos.size:]), "skip": skipped / qk.numel(),
                          "rejected_indexed": f.stats()["n_rejected_indexed"]}
     t, u = out["trained"], out["untrained"]
-    assert t["auc"] > 0.9 and t["auc"] > u["auc"] + 0.2, out
-    assert t["rejected_indexed"] < 0.8 * u["rejected_indexed"], out
-    assert t["skip"] > 0 and u["skip"] > 0, out
+    assert t["auc"] > 0.95 and t["auc"] > u["auc"] + 0.2, out
+    assert t["rejected_indexed"] < 0.5 * u["rejected_indexed"], out
+    assert t["skip"] > u["skip"], out
