@@ -287,6 +287,7 @@ extern "C" void sbwt_index_free(sbwt_index *ix) {
     cudaFree(ix->d_scan);
     cudaFree(ix->d_node);
     cudaFree(ix->d_sel);
+    cudaFree(ix->d_back);
     for (int i = 0; i < 2; i++) {
         ix->ws[i].release();
         if (ix->pipe_stream[i]) cudaStreamDestroy(ix->pipe_stream[i]);

@@ -116,6 +116,7 @@ struct sbwt_index {
     // backward-step structures (stream.cu): node bytes and select samples
     uint8_t *d_node = nullptr;
     uint32_t *d_sel = nullptr;
+    uint64_t *d_back = nullptr;  // backward table (stream.cuh, SBWT_BACK_TABLE)
     uint32_t sel_off[4] = {0, 0, 0, 0}, sel_n[4] = {0, 0, 0, 0};
     bool stream_ok = false;
     // launch shape

@@ -97,6 +97,18 @@ __global__ void node_nibbles_kernel(u32 n, u32 k, const u64 *__restrict__ code, 
     node[t] = (uint8_t)byte;
 }
 
+// Backward table: entry v = pred(v) | group_letters(pred(v)) << 32 (node 0: 0).
+__global__ void back_table_kernel(const StreamView sv, u64 *__restrict__ back) {
+    const u32 v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= sv.n) return;
+    u64 e = 0;
+    if (v) {
+        const u32 u0 = sv.pred(v);
+        if (u0 < sv.n) e = (u64)u0 | ((u64)sv.group_letters(u0) << 32);
+    }
+    back[v] = e;
+}
+
 }  // namespace
 
 StreamView stream_view(const sbwt_index *ix) {
@@ -111,6 +123,7 @@ StreamView stream_view(const sbwt_index *ix) {
         sv.C[c] = (u32)ix->C[c];
     }
     sv.node = ix->d_node;
+    sv.back = ix->d_back;
     sv.n = (u32)ix->n;
     return sv;
 }
@@ -167,8 +180,12 @@ int build_stream(sbwt_index *ix, cudaStream_t s) {
             cur ^= 1;
         }
         node_nibbles_kernel<<<(n / 2 + 1 + 255) / 256, 256, 0, s>>>(n, ix->k, code[cur], len[cur], ix->d_node);
+        if (SBWT_BACK_TABLE) {
+            e = cudaMalloc(&ix->d_back, (size_t)n * sizeof(u64));
+            if (e == cudaSuccess) back_table_kernel<<<blocks, 256, 0, s>>>(stream_view(ix), ix->d_back);
+        }
         unsigned long long h_bad = 0;
-        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaMemcpyAsync(&h_bad, bad, sizeof h_bad, cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) fail(e);
@@ -183,8 +200,10 @@ int build_stream(sbwt_index *ix, cudaStream_t s) {
     if (rc) {
         cudaFree(ix->d_node);
         cudaFree(ix->d_sel);
+        cudaFree(ix->d_back);
         ix->d_node = nullptr;
         ix->d_sel = nullptr;
+        ix->d_back = nullptr;
         return rc;
     }
     ix->stream_ok = true;

@@ -25,6 +25,12 @@ constexpr u32 kSelLog = 6;          // one select sample per 64 ones
 constexpr uint8_t kGroupStart = 8;  // node nibble: bit 3 = first node of its group
 constexpr u32 kNoNode = 0;          // node 0 (the all-$ root) is never a k-mer's node
 
+// Backward steps through the 8-byte-per-column backward table (1) or through
+// select + node nibbles (0).
+#ifndef SBWT_BACK_TABLE
+#define SBWT_BACK_TABLE 1
+#endif
+
 // Position of the (i+1)-th one (0-based i) of the 64-bit MSB-first word w.
 __device__ __forceinline__ u32 msb_select(u64 w, u32 i) {
     u32 pos = 0;
@@ -82,6 +88,7 @@ struct StreamView {
     u32 sel_off[4];
     u32 sel_n[4];
     const uint8_t *node;   // per node a nibble (first letter | kGroupStart), two per byte
+    const u64 *back;       // backward table: per node pred(v) | group_letters(pred(v)) << 32
     u32 n;                 // nodes
     u32 C[4];
 
@@ -96,6 +103,30 @@ struct StreamView {
         return line_select(lines + (u64)b * lpc, lpc, sel + sel_off[b], sel_n[b], v - cb);
     }
 
+    // Letters present as first letters in the group that starts at u0 (bit 0 = $, bit 1 + c = letter c).
+    __device__ __forceinline__ u32 group_letters(u32 u0) const {
+        u32 m = 0;
+        u32 u = u0;
+#pragma unroll 1
+        for (u32 g = 0; g < 5u && u < n; g++, u++) {
+            const u32 f = (u32)(__ldg(node + (u >> 1)) >> ((u & 1u) << 2)) & 15u;
+            if (g && (f & kGroupStart)) break;
+            m |= 1u << (f & 7u);
+        }
+        return m;
+    }
+
+#if SBWT_BACK_TABLE
+    // Node of the k-mer a.y given the node v of the k-mer y.b, or kNoNode: one
+    // load of v's entry u0 | group_letters(u0) << 32 (the backward table); the
+    // member with first letter a sits after the members with smaller ones.
+    __device__ __forceinline__ u32 back_step(u32 v, u32 a) const {
+        const u64 e = __ldg(reinterpret_cast<const unsigned long long *>(back) + v);
+        const u32 m = (u32)(e >> 32);
+        if (!((m >> (a + 1u)) & 1u)) return kNoNode;
+        return (u32)e + (u32)__popc(m & ((1u << (a + 1u)) - 1u));
+    }
+#else
     // Node of the k-mer a.y given the node v of the k-mer y.b, or kNoNode.
     __device__ __forceinline__ u32 back_step(u32 v, u32 a) const {
         u32 u = pred(v);
@@ -111,6 +142,7 @@ struct StreamView {
         }
         return kNoNode;
     }
+#endif
 };
 
 }  // namespace dev
