@@ -355,7 +355,14 @@ __global__ void __launch_bounds__(128) search_queue_kernel(const R rk, const Sea
 // k-mer (backward step, or letters + presearch entry followed by its first
 // rank-pair step) or takes one rank-pair step.
 
-constexpr u32 kWin = 32;            // k-mers per window (granularity of chunk_row)
+// k-mers per window (a multiple of 32; also the granularity of chunk_row and
+// the longest run).  Longer runs mean fewer fresh searches per read (one per
+// run start, plus one per absent stretch) and a longer walk per lane.
+#ifndef SBWT_RUNS_WINDOW
+#define SBWT_RUNS_WINDOW 32
+#endif
+constexpr u32 kWin = SBWT_RUNS_WINDOW;
+static_assert(kWin % 32 == 0, "windows cover whole bitmap words");
 
 // Resident 128-thread blocks per SM the run-walking kernel is compiled for
 // (a register cap), measured on the large workload: 9 for the line ranker
@@ -415,7 +422,8 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
                     pe = min(pj + kWin, end);
                     if (pj < pe) {
                         prow = a.chunk_row[pj / kWin];
-                        if (member) member[pj / 32u] = 0u;  // kWin = 32: one word per window
+                        if (member)
+                            for (u64 w = pj / 32u; w < (pe + 31u) / 32u; w++) member[w] = 0u;
                     }
                 }
                 __syncwarp();
