@@ -52,30 +52,40 @@ int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, con
     if (n_rows == 0) return 0;
     if (!letters || !row_starts || (n_kmers && !answers && !member)) return set_error("NULL host pointer");
     if (row_starts[n_rows] > n_letters) return set_error("row_starts[n_rows] exceeds n_letters");
-    for (u64 r = 0; r < n_rows; r++)
-        if (row_starts[r + 1] < row_starts[r]) return set_error("row_starts must be non-decreasing (row %llu)",
-                                                                (unsigned long long)r);
     const u32 k = ix->k;
-    // chunks of whole rows
+    // validation and the k-mer total, threaded (this host work precedes every copy)
+    int64_t bad_row = -1;
+    u64 kk = 0;
+#pragma omp parallel for schedule(static) reduction(+ : kk) reduction(max : bad_row)
+    for (int64_t r = 0; r < (int64_t)n_rows; r++) {
+        const u64 a = row_starts[r], b = row_starts[r + 1];
+        if (b < a) bad_row = std::max<int64_t>(bad_row, r);
+        else kk += b - a >= k ? b - a - k + 1 : 0;
+    }
+    if (bad_row >= 0)
+        return set_error("row_starts must be non-decreasing (row %lld)", (long long)bad_row);
+    if (kk != n_kmers)
+        return set_error("n_kmers = %llu but the rows hold %llu k-mers", (unsigned long long)n_kmers,
+                         (unsigned long long)kk);
+    // chunks of whole rows: the end of each is found by binary search in the sorted row starts
     std::vector<Chunk> chunks;
     {
-        Chunk c{0, 0, row_starts[0], row_starts[0], 0, 0};
-        u64 kk = 0;
-        for (u64 r = 0; r < n_rows; r++) {
-            const u64 len = row_starts[r + 1] - row_starts[r];
-            const u64 nk = len >= k ? len - k + 1 : 0;
-            c.r1 = r + 1;
-            c.l1 = row_starts[r + 1];
-            c.nk += nk;
-            kk += nk;
-            if (c.l1 - c.l0 >= kChunkLetters || r + 1 == n_rows) {
-                chunks.push_back(c);
-                c = Chunk{r + 1, r + 1, row_starts[r + 1], row_starts[r + 1], kk, 0};
+        u64 r0 = 0, k0 = 0;
+        while (r0 < n_rows) {
+            const u64 *first = row_starts + r0 + 1, *last = row_starts + n_rows + 1;
+            // first row end at or past kChunkLetters letters; at least one row per chunk
+            u64 r1 = (u64)(std::lower_bound(first, last, row_starts[r0] + kChunkLetters) - row_starts);
+            r1 = std::min<u64>(std::max<u64>(r1, r0 + 1), n_rows);
+            u64 nk = 0;
+#pragma omp parallel for schedule(static) reduction(+ : nk) if (r1 - r0 > (1u << 16))
+            for (int64_t r = (int64_t)r0; r < (int64_t)r1; r++) {
+                const u64 len = row_starts[r + 1] - row_starts[r];
+                nk += len >= k ? len - k + 1 : 0;
             }
+            chunks.push_back(Chunk{r0, r1, row_starts[r0], row_starts[r1], k0, nk});
+            k0 += nk;
+            r0 = r1;
         }
-        if (kk != n_kmers)
-            return set_error("n_kmers = %llu but the rows hold %llu k-mers", (unsigned long long)n_kmers,
-                             (unsigned long long)kk);
     }
     SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
     for (int i = 0; i < 2; i++)
@@ -140,7 +150,9 @@ int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, con
         Workspace &w = ix->ws[slot];
         SBWT_TRY(drain(slot));  // slot's previous chunk has finished with its buffers
         const u64 nr = c.r1 - c.r0, nl = c.l1 - c.l0;
-        for (u64 r = 0; r <= nr; r++) w.h_rows[r] = row_starts[c.r0 + r] - c.l0;
+        uint64_t *hr = w.h_rows;
+#pragma omp parallel for schedule(static) if (nr > (1u << 16))
+        for (int64_t r = 0; r <= (int64_t)nr; r++) hr[r] = row_starts[c.r0 + r] - c.l0;
         SBWT_CHECK_CUDA(cudaMemcpyAsync(w.rows, w.h_rows, (nr + 1) * sizeof(u64), cudaMemcpyHostToDevice, s));
         if (pin_in) {
             SBWT_CHECK_CUDA(cudaMemcpyAsync(w.letters, letters + c.l0, nl, cudaMemcpyHostToDevice, s));

@@ -135,8 +135,11 @@ def _auc(pos, neg):
 def test_trained_network_gains_over_the_untrained_one(trained, cuda):
     """What training buys over the same sandwich with the untrained (initial) network, at the
     same threshold and Bloom settings: the trained network separates indexed k-mers from random
-    ones (AUC), sends far fewer indexed k-mers to the backup Bloom filter (a smaller filter for
-    the same false-positive rate) and skips more of a 90%-negative query set."""
+    ones (AUC) and sends far fewer indexed k-mers to the backup Bloom filter, so the filter that
+    keeps the sandwich exact is many times smaller for the same false-positive rate.  (The
+    untrained network rejects about half of everything at random, so its sandwich skips a
+    similar share of a 90%-negative query set, but only by carrying most of the index in its
+    Bloom filter.)"""
     import torch
     ix, pf, k = trained["ix"], trained["pf"], trained["k"]
     with sg.Prefilter.train(ix, steps=0, batch=2048, n_positive=400_000, n_negative=400_000, seed=9) as base:
@@ -159,5 +162,5 @@ def test_trained_network_gains_over_the_untrained_one(trained, cuda):
                          "rejected_indexed": f.stats()["n_rejected_indexed"]}
     t, u = out["trained"], out["untrained"]
     assert t["auc"] > 0.95 and t["auc"] > u["auc"] + 0.2, out
-    assert t["rejected_indexed"] < 0.5 * u["rejected_indexed"], out
-    assert t["skip"] > u["skip"], out
+    assert t["rejected_indexed"] < 0.25 * u["rejected_indexed"], out
+    assert t["skip"] > 0.3 and u["skip"] > 0, out
