@@ -67,10 +67,10 @@ typedef struct {
  *   fails after m letters, those m letters are in no indexed k-mer, so the
  *   k-m+1 k-mers containing them are answered absent without a search.
  * STREAM: SKIP_ABSENT, and after a k-mer is found the k-mer one letter to its
- *   left is reached by one backward step (a select and a look at the <= 5
- *   nodes of one suffix group) instead of a new search.  Needs the line
- *   layout's index size limit and four bits per column plus select samples,
- *   built on the GPU when the mode is selected. */
+ *   left is reached by one backward step (one load from a per-column table
+ *   of predecessor groups) instead of a new search.  Needs the line layout's
+ *   index size limit and about 8.6 bytes per column, built on the GPU when
+ *   the mode is selected. */
 #define SBWT_SEARCH_EVERY_KMER 0
 #define SBWT_SEARCH_SKIP_ABSENT 1
 #define SBWT_SEARCH_STREAM 2
