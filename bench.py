@@ -339,6 +339,7 @@ def main():
     kernel = ("search_runs_kernel" + ("<stream>" if args.search_mode == "stream" else "<skip>") if runs_form
               else ("search_queue_kernel" if args.kpt == 0 else "search_kernel"))
     load_s = time.perf_counter() - t
+    build_times = ix.build_times()  # device ms: rank words (lines), poppy, presearch, backward table
     info = ix.info()
 
     d_letters = torch.from_numpy(letters).to(dev)
@@ -513,6 +514,7 @@ def main():
                     letters.nbytes / 1e9, n_kmers * 8 / 1e9),
                 "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                 "index_build_s": round(build_s, 2), "index_builder": "gpu (sbwt_build_gpu, incl. host copies)", "index_load_s": round(load_s, 2),
+                "index_build_device_ms": {kk: round(vv, 3) for kk, vv in build_times.items()},
             },
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": f"of {peak_kind}",

@@ -114,6 +114,13 @@ int sbwt_index_info(const sbwt_index *index, uint64_t *n_bits, uint64_t C[5], ui
  * (include/gpu/presearch_kernel.hpp:19-37). */
 int sbwt_presearch(sbwt_index *index, uint32_t p);
 
+/* Device time in ms of the index's last build phases: ms[0] the line layout
+ * (rank words), ms[1] the poppy L0/L12 structures (0 if not built), ms[2]
+ * the presearch table (its last build), ms[3] the backward-step structures.
+ * The reference prints its presearch time (include/matrix_sbwt.hpp:188) and
+ * builds its rank structures on the CPU (rank_data_structures.hpp:142-198). */
+int sbwt_build_times(const sbwt_index *index, float ms[4]);
+
 /* Copies the presearch table to the host in the reference's format: two
  * arrays node_lefts[4^p], node_rights[4^p] (include/gpu/device_memory.hpp:
  * 136-138). */

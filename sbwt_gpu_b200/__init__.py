@@ -144,6 +144,12 @@ class Index:
         check(lib.sbwt_configure(self._h, layout, bits_in_superblock, rank_structure, int(with_shuffles),
                                  kmers_per_thread, threads_per_kmer, threads_per_block))
 
+    def build_times(self):
+        """Device ms of the last build phases: lines, poppy, presearch table, backward-step structures."""
+        ms = (ctypes.c_float * 4)()
+        check(lib.sbwt_build_times(self._h, ms))
+        return {"lines_ms": ms[0], "poppy_ms": ms[1], "presearch_ms": ms[2], "backward_ms": ms[3]}
+
     def set_search_mode(self, mode):
         """SEARCH_EVERY_KMER, SEARCH_SKIP_ABSENT or SEARCH_STREAM (default) for searches of reads;
         the answers are the same in every mode."""

@@ -114,12 +114,23 @@ int finish_index(sbwt_index *ix, const u64 *const words[4], const sbwt_params *p
     }
     cudaStream_t s = 0;
     u64 ones[4] = {0, 0, 0, 0};
+    // device time of each build phase (sbwt_build_times)
+    cudaEvent_t ev[5];
+    for (auto &e : ev) SBWT_CHECK_CUDA(cudaEventCreate(&e));
+    struct EvFree {
+        cudaEvent_t *e;
+        ~EvFree() {
+            for (int i = 0; i < 5; i++) cudaEventDestroy(e[i]);
+        }
+    } ev_free{ev};
+    SBWT_CHECK_CUDA(cudaEventRecord(ev[0], s));
     if (n / sbwt::dev::kLineBits + 1 <= sbwt::dev::kMaxLinesPerChar) {
         ix->lpc = (u32)(((n / sbwt::dev::kLineBits + 1) + 7) / 8 * 8);
         SBWT_CHECK_CUDA(cudaMalloc(&ix->d_lines, 4ull * ix->lpc * sizeof(ulonglong4)));
         SBWT_TRY(sbwt::build_lines(ix, s, ones));
         ix->lines_ok = true;
     }
+    SBWT_CHECK_CUDA(cudaEventRecord(ev[1], s));
     const bool want_poppy = prm->layout == SBWT_LAYOUT_POPPY || !ix->lines_ok;
     if (want_poppy) {
         SBWT_TRY(sbwt::build_poppy(ix, prm->bits_in_superblock, prm->rank_structure, s));
@@ -146,9 +157,13 @@ int finish_index(sbwt_index *ix, const u64 *const words[4], const sbwt_params *p
                          (unsigned long long)ix->C[4], (unsigned long long)n);
     apply_shape(ix, prm);
     if (ix->shape.layout == SBWT_LAYOUT_LINES && !ix->lines_ok) ix->shape.layout = SBWT_LAYOUT_POPPY;
+    SBWT_CHECK_CUDA(cudaEventRecord(ev[2], s));
     SBWT_TRY(sbwt::run_presearch(ix, prm->k_presearch, s));
+    SBWT_CHECK_CUDA(cudaEventRecord(ev[3], s));
     if (ix->shape.mode == SBWT_SEARCH_STREAM && ix->lines_ok) SBWT_TRY(sbwt::build_stream(ix, s));
+    SBWT_CHECK_CUDA(cudaEventRecord(ev[4], s));
     SBWT_CHECK_CUDA(cudaDeviceSynchronize());
+    for (int i = 0; i < 4; i++) SBWT_CHECK_CUDA(cudaEventElapsedTime(&ix->build_ms[i], ev[i], ev[i + 1]));
     return 0;
 }
 
@@ -311,7 +326,23 @@ extern "C" int sbwt_presearch(sbwt_index *ix, uint32_t p) {
     clear_error();
     if (!ix) return set_error("index is NULL");
     SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
-    return run_presearch(ix, p, 0);
+    cudaEvent_t e0, e1;
+    SBWT_CHECK_CUDA(cudaEventCreate(&e0));
+    SBWT_CHECK_CUDA(cudaEventCreate(&e1));
+    cudaEventRecord(e0, 0);
+    const int rc = run_presearch(ix, p, 0);
+    cudaEventRecord(e1, 0);
+    if (rc == 0 && cudaEventSynchronize(e1) == cudaSuccess) cudaEventElapsedTime(&ix->build_ms[2], e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
+
+extern "C" int sbwt_build_times(const sbwt_index *ix, float ms[4]) {
+    clear_error();
+    if (!ix || !ms) return set_error("NULL argument");
+    std::memcpy(ms, ix->build_ms, sizeof(ix->build_ms));
+    return 0;
 }
 
 extern "C" int sbwt_presearch_export(const sbwt_index *ix, uint64_t *lefts, uint64_t *rights, uint64_t count) {

@@ -119,6 +119,8 @@ struct sbwt_index {
     uint64_t *d_back = nullptr;  // backward table (stream.cuh, SBWT_BACK_TABLE)
     uint32_t sel_off[4] = {0, 0, 0, 0}, sel_n[4] = {0, 0, 0, 0};
     bool stream_ok = false;
+    // device ms of the last build of: lines, poppy, presearch table, backward-step structures
+    float build_ms[4] = {0, 0, 0, 0};
     // launch shape
     sbwt::KernelShape shape;
     // scan block sums of the rank builds

@@ -482,3 +482,12 @@ def test_host_pipelines_across_chunks(small, cuda):
     assert letters.size > (64 << 20)
     assert np.array_equal(host, want)
     assert np.array_equal(mem, _bits_of(want))
+
+
+def test_build_times_reported(small, cuda):
+    b = small["built"]
+    with sg.Index.from_bits(b.bits, b.n_bits, k=31, k_presearch=10) as ix:
+        t = ix.build_times()
+        assert t["lines_ms"] > 0 and t["presearch_ms"] > 0 and t["backward_ms"] > 0 and t["poppy_ms"] == 0
+        ix.presearch(12)
+        assert ix.build_times()["presearch_ms"] > 0
