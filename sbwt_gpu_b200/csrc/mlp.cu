@@ -101,10 +101,11 @@ __global__ void __launch_bounds__(128) gemm_tn_kernel(const bf16 *__restrict__ A
 
 constexpr u32 kInferSmem = kHid * kIn * 2 + kHid * kHid * 2 + kTileM * kIn * 2;  // 224 KiB
 
-__device__ __forceinline__ void onehot_row(uint8_t *tile, u32 R, u32 r, u64 kmer, u32 k) {
-    // chunk q holds inputs 8q..8q+7 = letters 2q and 2q+1 (4 one-hot inputs each)
+// One-hot chunks q0..q1-1 of row r: chunk q holds inputs 8q..8q+7 = letters
+// 2q and 2q+1 (4 one-hot inputs each).
+__device__ __forceinline__ void onehot_chunks(uint8_t *tile, u32 R, u32 r, u64 kmer, u32 k, u32 q0, u32 q1) {
 #pragma unroll
-    for (u32 q = 0; q < kIn / 8; q++) {
+    for (u32 q = q0; q < q1; q++) {
         const u32 i0 = 2 * q, i1 = 2 * q + 1;
         const u32 c0 = i0 < k ? letter(kmer, i0) : 4u;
         const u32 c1 = i1 < k ? letter(kmer, i1) : 4u;
@@ -118,9 +119,17 @@ __device__ __forceinline__ void onehot_row(uint8_t *tile, u32 R, u32 r, u64 kmer
     }
 }
 
-// One CTA per SM (224 KiB of shared memory, all 512 TMEM columns), 128
-// threads; thread t owns row t of every 128-k-mer tile.
-__global__ void __launch_bounds__(128, 1)
+// One CTA per SM (224 KiB of shared memory, all 512 TMEM columns), 512
+// threads = 16 warps.  Warp w reaches TMEM lanes 32*(w%4)..+31 (rows of the
+// 128-k-mer tile) and handles hidden columns 64*(w/4)..+63 of them in both
+// epilogues, so four warps share each row and the epilogues run on all 16
+// warps; layer 2's 256 -> 1 dot is summed over the four column groups in
+// shared memory (the one-hot tile's space, free once layer 1 has run).
+constexpr u32 kInferThreads = 512;
+constexpr u32 kColGroups = kInferThreads / kTileM;  // 4
+constexpr u32 kGroupCols = kHid / kColGroups;       // 64
+
+__global__ void __launch_bounds__(kInferThreads, 1)
     mlp_infer_kernel(const u64 *__restrict__ kmers, u64 n, u32 k, const bf16 *__restrict__ W1b,
                      const bf16 *__restrict__ W2b, const float *__restrict__ b1, const float *__restrict__ b2,
                      const float *__restrict__ w3, const float *__restrict__ b3, float *__restrict__ logits, int *err) {
@@ -130,14 +139,18 @@ __global__ void __launch_bounds__(128, 1)
     uint8_t *sW1 = smem;
     uint8_t *sW2 = smem + kHid * kIn * 2;
     uint8_t *sX = sW2 + kHid * kHid * 2;
+    float *sRed = reinterpret_cast<float *>(sX);  // [kColGroups][kTileM] partial dots (after layer 1)
     const u32 tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+    const u32 quarter = warp & 3u, cg = warp >> 2;
+    const u32 trow = quarter * 32u + lane;  // this thread's row of the tile
+    const u32 c0 = cg * kGroupCols;         // its first hidden column
     // weights into the canonical K-major layouts (once per launch)
-    for (u32 i = tid; i < kHid * (kIn / 8); i += 128u) {
+    for (u32 i = tid; i < kHid * (kIn / 8); i += kInferThreads) {
         const u32 r = i / (kIn / 8), kc = i % (kIn / 8);
         *reinterpret_cast<uint4 *>(sW1 + canon_offset(kHid, r, kc * 8)) =
             *reinterpret_cast<const uint4 *>(W1b + (size_t)r * kIn + kc * 8);
     }
-    for (u32 i = tid; i < kHid * (kHid / 8); i += 128u) {
+    for (u32 i = tid; i < kHid * (kHid / 8); i += kInferThreads) {
         const u32 r = i / (kHid / 8), kc = i % (kHid / 8);
         *reinterpret_cast<uint4 *>(sW2 + canon_offset(kHid, r, kc * 8)) =
             *reinterpret_cast<const uint4 *>(W2b + (size_t)r * kHid + kc * 8);
@@ -149,14 +162,19 @@ __global__ void __launch_bounds__(128, 1)
     fence_after_sync();
     const u32 tD = tmem_s;          // columns [0, 256): layer accumulators
     const u32 tA2 = tmem_s + 256u;  // columns [256, 384): layer-1 activations, BF16 pairs
-    const u32 lane_base = (warp * 32u) << 16;
+    const u32 lane_base = (quarter * 32u) << 16;
     const float bias3 = __ldg(b3);
     u32 phase = 0;
     bool ok = true;
     for (u64 tile = blockIdx.x; ok && tile * kTileM < n; tile += gridDim.x) {
-        const u64 row = tile * kTileM + tid;
-        const u64 kmer = row < n ? kmers[row] : 0ull;
-        onehot_row(sX, kTileM, tid, kmer, k);
+        {
+            // one-hot tile: thread (row tid % 128, chunk group tid / 128)
+            const u32 r = tid & (kTileM - 1u), g = tid / kTileM;
+            const u64 row = tile * kTileM + r;
+            const u64 kmer = row < n ? kmers[row] : 0ull;
+            constexpr u32 kChunks = kIn / 8 / kColGroups;  // 4 of the 16 chunks of a row
+            onehot_chunks(sX, kTileM, r, kmer, k, g * kChunks, (g + 1) * kChunks);
+        }
         fence_smem_to_async();
         __syncthreads();
         if (tid == 0) {
@@ -173,19 +191,25 @@ __global__ void __launch_bounds__(128, 1)
         phase ^= 1u;
         fence_after_sync();
         if (!__syncthreads_and(got)) { ok = false; break; }
-        // layer-1 epilogue: bias, ReLU, BF16, into TMEM as layer 2's A operand
-        for (u32 c = 0; c < kHid; c += 16) {
-            u32 v[16];
-            tmem_ld16(tD + lane_base + c, v);
-            tmem_wait_ld();
-            u32 packed[8];
+        // layer-1 epilogue on this thread's 64 columns: bias, ReLU, BF16, into TMEM as layer 2's A
+        {
+            u32 v[4][16];
 #pragma unroll
-            for (int j = 0; j < 16; j += 2) {
-                const float h0 = fmaxf(__uint_as_float(v[j]) + __ldg(b1 + c + j), 0.0f);
-                const float h1 = fmaxf(__uint_as_float(v[j + 1]) + __ldg(b1 + c + j + 1), 0.0f);
-                packed[j / 2] = pack_bf16x2(h0, h1);
+            for (u32 j = 0; j < 4; j++) tmem_ld16(tD + lane_base + c0 + 16u * j, v[j]);
+            tmem_wait_ld();
+#pragma unroll
+            for (u32 j = 0; j < 4; j++) {
+                tmem_tie(v[j]);
+                u32 packed[8];
+#pragma unroll
+                for (int t = 0; t < 16; t += 2) {
+                    const u32 c = c0 + 16u * j + t;
+                    const float h0 = fmaxf(__uint_as_float(v[j][t]) + __ldg(b1 + c), 0.0f);
+                    const float h1 = fmaxf(__uint_as_float(v[j][t + 1]) + __ldg(b1 + c + 1), 0.0f);
+                    packed[t / 2] = pack_bf16x2(h0, h1);
+                }
+                tmem_st8(tA2 + lane_base + (c0 + 16u * j) / 2u, packed);
             }
-            tmem_st8(tA2 + lane_base + c / 2, packed);
         }
         tmem_wait_st();
         fence_before_sync();
@@ -203,19 +227,33 @@ __global__ void __launch_bounds__(128, 1)
         phase ^= 1u;
         fence_after_sync();
         if (!__syncthreads_and(got)) { ok = false; break; }
-        // layer-2 epilogue: bias, ReLU, BF16 activation, dot with w3
-        float acc = 0.0f;
-        for (u32 c = 0; c < kHid; c += 16) {
-            u32 v[16];
-            tmem_ld16(tD + lane_base + c, v);
-            tmem_wait_ld();
+        // layer-2 epilogue: bias, ReLU, BF16 activation, partial dot with w3 over 64 columns
+        {
+            u32 v[4][16];
 #pragma unroll
-            for (int j = 0; j < 16; j++) {
-                const float h = bf16_round(fmaxf(__uint_as_float(v[j]) + __ldg(b2 + c + j), 0.0f));
-                acc = fmaf(h, __ldg(w3 + c + j), acc);
+            for (u32 j = 0; j < 4; j++) tmem_ld16(tD + lane_base + c0 + 16u * j, v[j]);
+            tmem_wait_ld();
+            float acc = 0.0f;
+#pragma unroll
+            for (u32 j = 0; j < 4; j++) {
+                tmem_tie(v[j]);
+#pragma unroll
+                for (int t = 0; t < 16; t++) {
+                    const u32 c = c0 + 16u * j + t;
+                    const float h = bf16_round(fmaxf(__uint_as_float(v[j][t]) + __ldg(b2 + c), 0.0f));
+                    acc = fmaf(h, __ldg(w3 + c), acc);
+                }
             }
+            sRed[cg * kTileM + trow] = acc;
         }
-        if (row < n) logits[row] = acc + bias3;
+        __syncthreads();
+        if (cg == 0) {
+            const u64 row = tile * kTileM + trow;
+            float sum = 0.0f;
+#pragma unroll
+            for (u32 g = 0; g < kColGroups; g++) sum += sRed[g * kTileM + trow];
+            if (row < n) logits[row] = sum + bias3;
+        }
         fence_before_sync();
         __syncthreads();
         fence_after_sync();
@@ -535,7 +573,7 @@ int infer(const u64 *kmers, u64 n, u32 k, const bf16 *W1b, const bf16 *W2b, cons
     }
     const u64 tiles = (n + kTileM - 1) / kTileM;
     const u32 grid = (u32)std::min<u64>(tiles, (u64)num_sms);
-    mlp_infer_kernel<<<grid, 128, kInferSmem, s>>>(kmers, n, k, W1b, W2b, theta + off.b1, theta + off.b2,
+    mlp_infer_kernel<<<grid, kInferThreads, kInferSmem, s>>>(kmers, n, k, W1b, W2b, theta + off.b1, theta + off.b2,
                                                    theta + off.w3, theta + off.b3, logits, err);
     SBWT_CHECK_CUDA(cudaGetLastError());
     return 0;

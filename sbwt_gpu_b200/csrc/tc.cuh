@@ -105,6 +105,18 @@ __device__ __forceinline__ void tmem_st8(u32 taddr, const u32 (&v)[8]) {
 }
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Orders the use of v after a preceding tmem_wait_ld (the registers of an
+// asynchronous TMEM load are only valid after the wait; this empty volatile
+// asm ties them to that point so the compiler cannot use them earlier).
+__device__ __forceinline__ void tmem_tie(u32 (&v)[16]) {
+    asm volatile(""
+                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
+                   "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]),
+                   "+r"(v[15])
+                 :
+                 : "memory");
+}
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 // ------------------------------------------------------------- MMA issue
