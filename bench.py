@@ -154,54 +154,67 @@ def measured_hbm():
 
 
 class Clocks:
-    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
-
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event (throttle) reasons of the benchmarked GPU, sampled every 10 ms by a
+    host thread through NVML (read-only queries) during the timed region; nvidia-smi's 200 ms loop
+    is too coarse for a timed region of tens of milliseconds."""
 
     def __init__(self, device_index):
         self.dev = device_index
-        self.proc = None
-        self.path = None
+        self.samples = []
+        self.thread = None
+        self.stop_flag = False
+
+    def _handle(self, nv):
+        import torch
+        pr = torch.cuda.get_device_properties(self.dev)
+        try:  # the GPU of this CUDA device, by PCI address (NVML numbers GPUs its own way)
+            return nv.nvmlDeviceGetHandleByPciBusId(f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0")
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.dev)
 
     def start(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
+        import threading
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._handle(nv)
+            smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        except Exception:
+            return
+        names = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                 "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                 "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                 "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+
+        def run():
+            while not self.stop_flag:
+                try:
+                    sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                    bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((sm, smax, [n for n, b in names.items() if bits & b]))
+                except Exception:
+                    pass
+                time.sleep(0.01)
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
+        t0 = time.perf_counter()
+        while not self.samples and time.perf_counter() - t0 < 2.0:  # sampling is live before timing starts
+            time.sleep(0.001)
 
     def stop(self):
-        if self.proc is None:
+        if self.thread is None:
             return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 8:
-                continue
-            try:
-                sm.append(float(f[0]))
-                smax.append(float(f[1]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[4:8]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        os.unlink(self.path)
-        if not sm:
+        self.stop_flag = True
+        self.thread.join(timeout=2)
+        if len(self.samples) > 1:
+            self.samples = self.samples[1:]  # the first sample predates the timed region
+        if not self.samples:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median(x[0] for x in self.samples),
+                "sm_max_mhz": max(x[1] for x in self.samples),
+                "reasons": sorted({r for x in self.samples for r in x[2]}), "samples": len(self.samples),
+                "source": "NVML every 10 ms"}
 
 
 def cpu_reference(ox, letters, rows, k, p, budget_s, table):

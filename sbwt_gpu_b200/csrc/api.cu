@@ -164,6 +164,8 @@ int finish_index(sbwt_index *ix, const u64 *const words[4], const sbwt_params *p
     SBWT_CHECK_CUDA(cudaEventRecord(ev[4], s));
     SBWT_CHECK_CUDA(cudaDeviceSynchronize());
     for (int i = 0; i < 4; i++) SBWT_CHECK_CUDA(cudaEventElapsedTime(&ix->build_ms[i], ev[i], ev[i + 1]));
+    if (!want_poppy) ix->build_ms[1] = 0.0f;
+    if (!ix->stream_ok) ix->build_ms[3] = 0.0f;
     return 0;
 }
 

@@ -120,7 +120,8 @@ __device__ __forceinline__ void onehot_chunks(uint8_t *tile, u32 R, u32 r, u64 k
 }
 
 // One CTA per SM (224 KiB of shared memory, all 512 TMEM columns), 512
-// threads = 16 warps.  Warp w reaches TMEM lanes 32*(w%4)..+31 (rows of the
+// threads = 16 warps.  b1, b2 and w3 must be 16-byte aligned (float4 loads;
+// their offsets in the parameter vector are multiples of 4 floats).  Warp w reaches TMEM lanes 32*(w%4)..+31 (rows of the
 // 128-k-mer tile) and handles hidden columns 64*(w/4)..+63 of them in both
 // epilogues, so four warps share each row and the epilogues run on all 16
 // warps; layer 2's 256 -> 1 dot is summed over the four column groups in
@@ -202,11 +203,13 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                 tmem_tie(v[j]);
                 u32 packed[8];
 #pragma unroll
-                for (int t = 0; t < 16; t += 2) {
-                    const u32 c = c0 + 16u * j + t;
-                    const float h0 = fmaxf(__uint_as_float(v[j][t]) + __ldg(b1 + c), 0.0f);
-                    const float h1 = fmaxf(__uint_as_float(v[j][t + 1]) + __ldg(b1 + c + 1), 0.0f);
-                    packed[t / 2] = pack_bf16x2(h0, h1);
+                for (int t = 0; t < 16; t += 4) {
+                    // the same 4 biases for every lane of the warp: one 16-byte load
+                    const float4 bb = __ldg(reinterpret_cast<const float4 *>(b1 + c0 + 16u * j + t));
+                    packed[t / 2] = pack_bf16x2(fmaxf(__uint_as_float(v[j][t]) + bb.x, 0.0f),
+                                                fmaxf(__uint_as_float(v[j][t + 1]) + bb.y, 0.0f));
+                    packed[t / 2 + 1] = pack_bf16x2(fmaxf(__uint_as_float(v[j][t + 2]) + bb.z, 0.0f),
+                                                    fmaxf(__uint_as_float(v[j][t + 3]) + bb.w, 0.0f));
                 }
                 tmem_st8(tA2 + lane_base + (c0 + 16u * j) / 2u, packed);
             }
@@ -238,10 +241,14 @@ __global__ void __launch_bounds__(kInferThreads, 1)
             for (u32 j = 0; j < 4; j++) {
                 tmem_tie(v[j]);
 #pragma unroll
-                for (int t = 0; t < 16; t++) {
+                for (int t = 0; t < 16; t += 4) {
                     const u32 c = c0 + 16u * j + t;
-                    const float h = bf16_round(fmaxf(__uint_as_float(v[j][t]) + __ldg(b2 + c), 0.0f));
-                    acc = fmaf(h, __ldg(w3 + c), acc);
+                    const float4 bb = __ldg(reinterpret_cast<const float4 *>(b2 + c));
+                    const float4 ww = __ldg(reinterpret_cast<const float4 *>(w3 + c));
+                    acc = fmaf(bf16_round(fmaxf(__uint_as_float(v[j][t]) + bb.x, 0.0f)), ww.x, acc);
+                    acc = fmaf(bf16_round(fmaxf(__uint_as_float(v[j][t + 1]) + bb.y, 0.0f)), ww.y, acc);
+                    acc = fmaf(bf16_round(fmaxf(__uint_as_float(v[j][t + 2]) + bb.z, 0.0f)), ww.z, acc);
+                    acc = fmaf(bf16_round(fmaxf(__uint_as_float(v[j][t + 3]) + bb.w, 0.0f)), ww.w, acc);
                 }
             }
             sRed[cg * kTileM + trow] = acc;
@@ -571,6 +578,8 @@ int infer(const u64 *kmers, u64 n, u32 k, const bf16 *W1b, const bf16 *W2b, cons
         SBWT_CHECK_CUDA(cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem));
         attr_set = true;
     }
+    for (const float *q : {theta + off.b1, theta + off.b2, theta + off.w3})
+        if ((uintptr_t)q & 15u) return set_error("MLP parameters must be 16-byte aligned");
     const u64 tiles = (n + kTileM - 1) / kTileM;
     const u32 grid = (u32)std::min<u64>(tiles, (u64)num_sms);
     mlp_infer_kernel<<<grid, kInferThreads, kInferSmem, s>>>(kmers, n, k, W1b, W2b, theta + off.b1, theta + off.b2,
