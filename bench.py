@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--tpb", type=int, default=0)
     ap.add_argument("--layout", choices=["lines", "poppy"], default="lines")
     ap.add_argument("--sb", type=int, default=1024, help="bits in superblock of the poppy layout")
+    ap.add_argument("--l2-fetch", type=int, default=0, choices=[0, 32, 64, 128],
+                    help="L2 fetch granularity in bytes for the searches (0: leave the device default)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-e2e", action="store_true")
@@ -352,6 +354,8 @@ def main():
     kernel = ("search_runs_kernel" + ("<stream>" if args.search_mode == "stream" else "<skip>") if runs_form
               else ("search_queue_kernel" if args.kpt == 0 else "search_kernel"))
     load_s = time.perf_counter() - t
+    if args.l2_fetch:
+        ix.set_l2_fetch_granularity(args.l2_fetch)
     build_times = ix.build_times()  # device ms: rank words (lines), poppy, presearch, backward table
     info = ix.info()
 
@@ -522,7 +526,7 @@ def main():
             "config": {
                 "workload": WORKLOADS[args.workload] if args.scale == 1.0 else f"{args.workload} x{args.scale}",
                 "n_kmers_per_gpu": n_kmers, "n_columns": info["n_bits"], "k": k, "p": p,
-                "layout": args.layout, "present_kmers": hits,
+                "layout": args.layout, "present_kmers": hits, "l2_fetch_bytes": args.l2_fetch or "default",
                 "l2": "inputs and outputs larger than L2 (letters %.2f GB, answers %.2f GB); no flush" % (
                     letters.nbytes / 1e9, n_kmers * 8 / 1e9),
                 "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
