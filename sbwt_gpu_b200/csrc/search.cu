@@ -366,13 +366,11 @@ __global__ void __launch_bounds__(128) search_queue_kernel(const R rk, const Sea
 constexpr u32 kWin = SBWT_RUNS_WINDOW;
 static_assert(kWin % 32 == 0, "windows cover whole bitmap words");
 
-// 1: a warp writes ~0 to all answers of its windows when it takes them
-// (coalesced) and found k-mers overwrite theirs; 0: every answer is written
-// once, by the lane that settles it (found, or absent by a failed search or
-// backward step), so found answers never rewrite part of a written sector.
-#ifndef SBWT_RUNS_PREFILL
-#define SBWT_RUNS_PREFILL 1
-#endif
+// Answers: a warp writes ~0 to all answers of its windows when it takes them
+// (coalesced) and found k-mers overwrite theirs.  (Writing each answer once,
+// by the lane that settles it, was measured 22 % slower on the large
+// workload: the skip's bursts of single 8-byte stores cost more than the
+// rewritten sectors.)
 
 // Resident 128-thread blocks per SM the run-walking kernel is compiled for
 // (a register cap), measured on the large workload: 9 for the line ranker
@@ -426,7 +424,7 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
                     more = false;
                 } else {
                     const u64 end = min((u64)base + 32u * kWin, n_eff);
-                    if (SBWT_RUNS_PREFILL && a.answers)  // NULL: membership bitmap only
+                    if (a.answers)  // NULL: membership bitmap only
                         for (u64 t = base + lane; t < end; t += 32u) a.answers[t] = ~0ull;
                     pj = min((u64)base + (u64)lane * kWin, end);
                     pe = min(pj + kWin, end);
@@ -522,10 +520,6 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
         if (found != ~0u) {
             if (a.answers) a.answers[J] = (u64)found;
             if (member) atomicOr(member + (J >> 5), 1u << (J & 31u));
-        } else if (!SBWT_RUNS_PREFILL && adv && a.answers) {
-            // the k-mers settled absent: J and the adv-1 to its left (within the run)
-            const u32 cnt = min(adv, left + 1u);
-            for (u32 t = 0; t < cnt; t++) a.answers[J - t] = ~0ull;
         }
         if (adv) {
             if (STREAM) V = found != ~0u ? found : dev::kNoNode;
