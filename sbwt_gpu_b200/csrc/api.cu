@@ -305,7 +305,7 @@ extern "C" void sbwt_index_free(sbwt_index *ix) {
     cudaFree(ix->d_node);
     cudaFree(ix->d_sel);
     cudaFree(ix->d_back);
-    for (int i = 0; i < 2; i++) {
+    for (int i = 0; i < sbwt_index::kPipeSlots; i++) {
         ix->ws[i].release();
         if (ix->pipe_stream[i]) cudaStreamDestroy(ix->pipe_stream[i]);
     }
@@ -622,7 +622,8 @@ extern "C" int sbwt_profile_read(sbwt_index *ix, sbwt_profile *out) {
 
 extern "C" uint64_t sbwt_count_kmers(const uint64_t *row_starts, uint64_t n_rows, uint32_t k) {
     uint64_t t = 0;
-    for (uint64_t r = 0; r < n_rows; r++) {
+#pragma omp parallel for schedule(static) reduction(+ : t) if (n_rows > (1u << 16))
+    for (int64_t r = 0; r < (int64_t)n_rows; r++) {
         const uint64_t len = row_starts[r + 1] - row_starts[r];
         if (len >= k) t += len - k + 1;
     }

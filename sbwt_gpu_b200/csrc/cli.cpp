@@ -215,7 +215,10 @@ int main(int argc, char **argv) {
     const int prc = parse(argc, argv, o);
     if (prc == 2) return 0;
     if (prc) return 1;
+    const auto t_main = std::chrono::steady_clock::now();
     cudaSetDevice(o.p.device);
+    cudaFree(nullptr);  // creates the CUDA context here, so that its cost is reported on its own
+    std::fprintf(stderr, "%f ms for creating the CUDA context.\n", ms_since(t_main));
     cudaDeviceSetLimit(cudaLimitMaxL2FetchGranularity, o.limit_presearch);  // presearch.hpp:34-37
     auto t0 = std::chrono::steady_clock::now();
     sbwt_index *ix = nullptr;
@@ -271,5 +274,6 @@ int main(int argc, char **argv) {
     if (!o.store) std::fprintf(stderr, "The results are not stored to the file.\n");
     sbwt_queries_free(&q);
     sbwt_index_free(ix);
+    std::fprintf(stderr, "%f ms in total, from the start of main.\n", ms_since(t_main));
     return rc;
 }

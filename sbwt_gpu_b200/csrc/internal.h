@@ -41,7 +41,7 @@ struct SearchArgs {
     u32 chunk;                    // k-mers per grab; with `runs`, k-mers per window of chunk_row
     u32 runs;                     // read mode: walk runs right to left with the absent-run skip
     u32 stream;                   // with `runs`: backward steps from a found k-mer (needs sv)
-    dev::StreamView sv;           // select samples + node bytes (stream.cuh)
+    dev::StreamView sv;           // backward table, node nibbles, select samples (stream.cuh)
     uint32_t *member;             // with `runs`: membership bitmap written by the search kernel, or NULL
     // k-mer list mode: k-mer j is kmer_list[j] (MSB-first word)
     const u64 *kmer_list;
@@ -113,7 +113,7 @@ struct sbwt_index {
     uint32_t p = 0;
     void *d_pre = nullptr;
     bool pre64 = false;
-    // backward-step structures (stream.cu): node bytes and select samples
+    // backward-step structures (stream.cu): node nibbles, select samples, backward table
     uint8_t *d_node = nullptr;
     uint32_t *d_sel = nullptr;
     uint64_t *d_back = nullptr;  // backward table (stream.cuh, SBWT_BACK_TABLE)
@@ -127,9 +127,10 @@ struct sbwt_index {
     uint64_t *d_scan = nullptr;
     size_t scan_cap = 0;
     // per-call work buffers: ws[0] serves the device-pointer entry points,
-    // ws[0] and ws[1] the two streams of the host pipeline
-    sbwt::Workspace ws[2];
-    cudaStream_t pipe_stream[2] = {nullptr, nullptr};
+    // ws[0 .. kPipeSlots) the streams of the host pipeline
+    static constexpr int kPipeSlots = 3;
+    sbwt::Workspace ws[kPipeSlots];
+    cudaStream_t pipe_stream[kPipeSlots] = {nullptr, nullptr, nullptr};
     // bumped whenever a device structure a search reads is rebuilt (graph keys)
     uint64_t gen = 1;
     bool use_graph = false;

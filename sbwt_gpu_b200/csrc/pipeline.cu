@@ -1,8 +1,9 @@
 // pipeline.cu -- sbwt_search_reads_host: a batch of reads in host memory is
-// streamed through the GPU in chunks of rows.  Two CUDA streams alternate;
-// on each, a chunk's letters and row table go host->device, the chunk is
-// packed and searched, and its answers come back device->host, so the copies
-// of one chunk overlap the search of the other.
+// streamed through the GPU in chunks of rows.  Three CUDA streams take
+// turns; on each, a chunk's letters and row table go host->device, the chunk
+// is packed and searched, and its answers come back device->host, so the
+// copies of one chunk overlap the search of another while the host prepares
+// the next.
 //
 // This replaces the strictly sequential host<->device chain of the reference
 // (KmerSearch::search, include/epicseq/kmer_search.hpp:97-160: one H2D of the
@@ -88,7 +89,8 @@ int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, con
         }
     }
     SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
-    for (int i = 0; i < 2; i++)
+    constexpr int kSlots = sbwt_index::kPipeSlots;
+    for (int i = 0; i < kSlots; i++)
         if (!ix->pipe_stream[i]) SBWT_CHECK_CUDA(cudaStreamCreateWithFlags(&ix->pipe_stream[i], cudaStreamNonBlocking));
     const bool pin_in = is_pinned(letters);
     const bool pin_out = answers && (n_kmers == 0 || is_pinned(answers));
@@ -99,7 +101,7 @@ int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, con
         max_k = std::max(max_k, c.nk);
     }
     const u64 max_words = (max_k + 31) / 32;
-    for (int i = 0; i < 2; i++) {
+    for (int i = 0; i < kSlots; i++) {
         Workspace &w = ix->ws[i];
         SBWT_TRY(grow(w.letters, w.letters_cap, max_letters + 16));
         SBWT_TRY(grow(w.rows, w.rows_cap, max_rows + 1));
@@ -115,7 +117,8 @@ int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, con
     }
     if (member) std::memset(member, 0, (n_kmers + 31) / 32 * sizeof(uint32_t));
     // pending[i]: chunk whose results sit in slot i's pinned staging
-    long pending[2] = {-1, -1};
+    long pending[kSlots];
+    for (long &x : pending) x = -1;
     auto drain = [&](int slot) -> int {
         SBWT_CHECK_CUDA(cudaStreamSynchronize(ix->pipe_stream[slot]));
         if (pending[slot] >= 0) {
@@ -144,7 +147,7 @@ int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, con
         return 0;
     };
     for (size_t b = 0; b < chunks.size(); b++) {
-        const int slot = (int)(b & 1);
+        const int slot = (int)(b % kSlots);
         const Chunk &c = chunks[b];
         cudaStream_t s = ix->pipe_stream[slot];
         Workspace &w = ix->ws[slot];
@@ -179,8 +182,7 @@ int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, con
             pending[slot] = (long)b;
         }
     }
-    SBWT_TRY(drain(0));
-    SBWT_TRY(drain(1));
+    for (size_t i = 0; i < (size_t)kSlots; i++) SBWT_TRY(drain((int)((chunks.size() + i) % kSlots)));
     return 0;
 }
 

@@ -1,6 +1,7 @@
-// stream.cu -- builds the node bytes and select samples of the backward step
-// (stream.cuh) on the GPU, from the index's lines alone, so that indexes
-// loaded from the reference's files get them too.  No reference counterpart.
+// stream.cu -- builds the backward-step structures (stream.cuh): select
+// samples, node nibbles and the backward table, on the GPU from the index's
+// lines alone, so that indexes loaded from the reference's files get them
+// too.  No reference counterpart.
 //
 // First letters and groups come from the labels: with pred(v) = the first
 // node of the group of v's predecessor (stream.cuh), the last letter of

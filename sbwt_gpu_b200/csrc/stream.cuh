@@ -13,8 +13,10 @@
 // select_b(v - C[b]) whose first letter is a, if there is one.  Per node the
 // engine keeps four bits, two nodes per byte (even node in the low half): its
 // first letter (0 = $, 1..4 = A..T) and a flag for the first node of its
-// group (bit 3).  select_c uses the line counts plus a
-// sample of the line holding every 64th one.
+// group (bit 3); and the backward table: per node v, pred(v) with the set of
+// first letters of pred(v)'s group, so that a backward step is one load.
+// select_c uses the line counts plus a sample of the line holding every 64th
+// one.
 #pragma once
 #include "device.cuh"
 
