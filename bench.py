@@ -478,6 +478,33 @@ def main():
         per_kmer = {"value": n_kmers * args.steps / (tt / 1e3), "ms_per_step": tt / args.steps,
                     "search_kernel_ms": statistics.mean(t_ms), "kernel": "search_queue_kernel"}
 
+    # ---- membership only on the device: no answer array, the kernel writes the bitmap alone
+    member_only = None
+    if runs_form and rank == 0:
+        ix.profile(True)
+        d_mem2 = torch.zeros_like(d_mem)
+
+        def mstep():
+            ix.search_reads(d_letters, d_rows, None, n_kmers, d_member_bits=d_mem2, stream=stream)
+
+        for _ in range(2):
+            mstep()
+        torch.cuda.synchronize(dev)
+        ev0.record(stream)
+        t_ms = []
+        for _ in range(args.steps):
+            mstep()
+            t_ms.append(ix.last_profile()["search_ms"])
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        tt = ev0.elapsed_time(ev1)
+        full = ans.size // 32
+        if not np.array_equal(d_mem2[:full].cpu().numpy().view(np.uint32), bits_of(ans)[:full]):
+            raise SystemExit("bench: membership bits differ from the oracle")
+        member_only = {"value": n_kmers * args.steps / (tt / 1e3), "ms_per_step": tt / args.steps,
+                       "search_kernel_ms": statistics.mean(t_ms), "output": "membership bitmap only (no answers)"}
+        del d_mem2
+
     # ---- autotuned leg: the tuner picks shape and presearch depth on a sample, then the batch is timed again
     tuned = None
     if not args.no_autotune and rank == 0:
@@ -544,6 +571,7 @@ def main():
             "gpu_launches": launches,
             "clocks": clk,
             "per_kmer": per_kmer,
+            "membership_only": member_only,
             "autotuned": tuned,
             "prefilter": prefilter,
         }
