@@ -53,6 +53,42 @@ __device__ __forceinline__ u64 ld_nc(const u64 *p) {
     return v;
 }
 
+// Gathers with little reuse (a presearch entry, a backward-table entry) are
+// read with an L2 evict-first policy, so that they do not push the lines of
+// the rank steps out of L2 (createpolicy and .L2::cache_hint: PTX ISA 7.4+,
+// sm_80+).  Build option SBWT_GATHER_EVICT_FIRST=0 reads them plainly.
+#ifndef SBWT_GATHER_EVICT_FIRST
+#define SBWT_GATHER_EVICT_FIRST 1
+#endif
+
+__device__ __forceinline__ u64 l2_evict_first_policy() {
+    u64 p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+__device__ __forceinline__ uint2 ld_gather_u32x2(const uint2 *p, u64 pol) {
+    uint2 v;
+#if SBWT_GATHER_EVICT_FIRST
+    asm("ld.global.nc.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;" : "=r"(v.x), "=r"(v.y) : "l"(p), "l"(pol));
+#else
+    (void)pol;
+    v = __ldg(p);
+#endif
+    return v;
+}
+
+__device__ __forceinline__ u64 ld_gather_u64(const u64 *p, u64 pol) {
+    u64 v;
+#if SBWT_GATHER_EVICT_FIRST
+    asm("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(p), "l"(pol));
+#else
+    (void)pol;
+    v = __ldg(reinterpret_cast<const unsigned long long *>(p));
+#endif
+    return v;
+}
+
 // x >> s with the PTX rule that s >= 64 gives 0 (the reference relies on it,
 // include/gpu/rank_kernel.hpp:218,226-229).
 __device__ __forceinline__ u64 shr_clamp(u64 x, u32 s) {
