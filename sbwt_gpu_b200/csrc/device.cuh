@@ -32,12 +32,26 @@ constexpr u32 kLineBits = 224;      // data bits per 32-byte line
 constexpr u32 kLineBytes = 32;
 constexpr u32 kMaxLinesPerChar = 1u << 24;  // 32-bit counts: 224 * 2^24 < 2^32
 
+// Build option SBWT_LINES_EVICT_LAST=1: lines are read with an L2
+// evict-last policy (kept in L2 ahead of other data).
+#ifndef SBWT_LINES_EVICT_LAST
+#define SBWT_LINES_EVICT_LAST 0
+#endif
+
 // 256-bit read-only load of one line (sm_100 supports .v4.u64 global loads).
 __device__ __forceinline__ ulonglong4 ld_line(const ulonglong4 *p) {
     ulonglong4 v;
+#if SBWT_LINES_EVICT_LAST
+    u64 pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    asm("ld.global.nc.L2::cache_hint.v4.u64 {%0, %1, %2, %3}, [%4], %5;"
+        : "=l"(v.x), "=l"(v.y), "=l"(v.z), "=l"(v.w)
+        : "l"(p), "l"(pol));
+#else
     asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];"
         : "=l"(v.x), "=l"(v.y), "=l"(v.z), "=l"(v.w)
         : "l"(p));
+#endif
     return v;
 }
 
