@@ -183,6 +183,9 @@ int new_index(const sbwt_params *prm, sbwt_index **out, sbwt_index **ix_out) {
     ix->k = prm->k;
     cudaDeviceGetAttribute(&ix->num_sms, cudaDevAttrMultiProcessorCount, prm->device);
     if (ix->num_sms <= 0) ix->num_sms = 1;
+    int l2 = 0;
+    cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, prm->device);
+    ix->l2_bytes = l2 > 0 ? (uint64_t)l2 : 0;
     *ix_out = ix;
     return 0;
 }
@@ -411,6 +414,15 @@ extern "C" int sbwt_set_search_mode(sbwt_index *ix, int32_t mode) {
 }
 
 namespace sbwt {
+
+bool index_exceeds_l2(const sbwt_index *ix) {
+    u64 bytes = ix->shape.layout == SBWT_LAYOUT_LINES ? 4ull * ix->lpc * 32ull
+                                                      : 4ull * (ix->wpv + ix->l0w + ix->l12w) * 8ull;
+    if (ix->p) bytes += (1ull << (2 * ix->p)) * (ix->pre64 ? 16ull : 8ull);
+    if (ix->d_back) bytes += ix->n * 8ull;
+    return bytes > ix->l2_bytes;
+}
+
 namespace {
 
 SearchArgs base_args(const sbwt_index *ix, bool rows) {
@@ -432,6 +444,7 @@ SearchArgs base_args(const sbwt_index *ix, bool rows) {
     a.runs = rows && runs_form(ix);
     a.stream = a.runs && stream_form(ix);
     if (a.stream) a.sv = stream_view(ix);
+    a.gather_evict_first = a.runs && index_exceeds_l2(ix);
     return a;
 }
 

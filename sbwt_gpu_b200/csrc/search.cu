@@ -412,7 +412,7 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
     u32 left = 0;                  // k-mers of the run left of J
     u32 L = 0, Rr = 0, I = kDone;
     u32 V = dev::kNoNode;          // STREAM: node of the k-mer right of J (found), or kNoNode
-    const u64 gpol = l2_evict_first_policy();  // for the presearch and backward-table gathers
+    const u64 gpol = l2_gather_policy(a.gather_evict_first);  // presearch and backward-table gathers
 
     for (;;) {
         // ---- fill: new windows once every lane's window is cut, then one run per lane
