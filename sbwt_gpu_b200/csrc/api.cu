@@ -415,12 +415,12 @@ extern "C" int sbwt_set_search_mode(sbwt_index *ix, int32_t mode) {
 
 namespace sbwt {
 
-bool index_exceeds_l2(const sbwt_index *ix) {
-    u64 bytes = ix->shape.layout == SBWT_LAYOUT_LINES ? 4ull * ix->lpc * 32ull
-                                                      : 4ull * (ix->wpv + ix->l0w + ix->l12w) * 8ull;
-    if (ix->p) bytes += (1ull << (2 * ix->p)) * (ix->pre64 ? 16ull : 8ull);
-    if (ix->d_back) bytes += ix->n * 8ull;
-    return bytes > ix->l2_bytes;
+void set_gather_policies(const sbwt_index *ix, SearchArgs &a) {
+    const u64 half = ix->l2_bytes / 2;
+    const u64 pre_bytes = ix->p ? (1ull << (2 * ix->p)) * (ix->pre64 ? 16ull : 8ull) : 0;
+    const u64 back_bytes = ix->d_back ? ix->n * 8ull : 0;
+    a.ef_pre = a.runs && pre_bytes > half;
+    a.ef_back = a.runs && back_bytes > half;
 }
 
 namespace {
@@ -444,7 +444,7 @@ SearchArgs base_args(const sbwt_index *ix, bool rows) {
     a.runs = rows && runs_form(ix);
     a.stream = a.runs && stream_form(ix);
     if (a.stream) a.sv = stream_view(ix);
-    a.gather_evict_first = a.runs && index_exceeds_l2(ix);
+    set_gather_policies(ix, a);
     return a;
 }
 

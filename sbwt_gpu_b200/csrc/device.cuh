@@ -67,13 +67,13 @@ __device__ __forceinline__ u64 ld_nc(const u64 *p) {
     return v;
 }
 
-// When the index is larger than L2, gathers with little reuse (a presearch
-// entry, a backward-table entry) are read with an L2 evict-first policy, so
-// that they do not push the lines of the rank steps out of L2; when it fits,
-// the policy is evict-normal (evict-first there makes them miss: measured
-// 28 % slower on an L2-resident index).  createpolicy and .L2::cache_hint:
-// PTX ISA 7.4+, sm_80+.  Build option SBWT_GATHER_EVICT_FIRST=0 reads them
-// plainly.
+// Gathers with little reuse (a presearch entry, a backward-table entry) from
+// a table too large to stay in L2 are read with an L2 evict-first policy, so
+// that they do not push the lines of the rank steps out of L2; gathers from a
+// table that fits use evict-normal (evict-first there makes them miss:
+// measured 28 % slower on an L2-resident index).  createpolicy and
+// .L2::cache_hint: PTX ISA 7.4+, sm_80+.  Build option
+// SBWT_GATHER_EVICT_FIRST=0 reads them plainly.
 #ifndef SBWT_GATHER_EVICT_FIRST
 #define SBWT_GATHER_EVICT_FIRST 1
 #endif

@@ -41,7 +41,8 @@ struct SearchArgs {
     u32 chunk;                    // k-mers per grab; with `runs`, k-mers per window of chunk_row
     u32 runs;                     // read mode: walk runs right to left with the absent-run skip
     u32 stream;                   // with `runs`: backward steps from a found k-mer (needs sv)
-    u32 gather_evict_first;       // with `runs`: the index exceeds L2 (gather policy, device.cuh)
+    u32 ef_pre, ef_back;          // with `runs`: evict-first gathers from the presearch / backward
+                                  // table (each set when that table cannot stay in L2; device.cuh)
     dev::StreamView sv;           // backward table, node nibbles, select samples (stream.cuh)
     uint32_t *member;             // with `runs`: membership bitmap written by the search kernel, or NULL
     // k-mer list mode: k-mer j is kmer_list[j] (MSB-first word)
@@ -175,9 +176,10 @@ template <class T> int grow_host(T *&p, size_t &cap, size_t need);
 
 // search.cu
 int launch_search(const sbwt_index *ix, SearchArgs &a, cudaStream_t s, uint32_t *launched_blocks);
-// Whether the structures the run walk gathers from (lines or poppy words,
-// presearch table, backward table) together exceed the device's L2.
-bool index_exceeds_l2(const sbwt_index *ix);
+// Evict-first policies for the run walk's gathers: a table gets one when it
+// is larger than half of the device's L2 (it cannot stay there next to the
+// lines).
+void set_gather_policies(const sbwt_index *ix, SearchArgs &a);
 // Whether a batch of reads searched with the index's current shape and mode
 // runs the run-walking kernel (absent-run skip), and whether it also takes
 // backward steps.

@@ -108,7 +108,7 @@ extern "C" int sbwt_search_reads_noalloc(sbwt_index *ix, const uint8_t *d_letter
     a.runs = runs_form(ix);
     a.stream = a.runs && stream_form(ix);
     if (a.stream) a.sv = stream_view(ix);
-    a.gather_evict_first = a.runs && index_exceeds_l2(ix);
+    set_gather_policies(ix, a);
     a.member = a.runs ? d_member_bits : nullptr;
     a.words = words;
     a.row_starts = d_row_starts;
