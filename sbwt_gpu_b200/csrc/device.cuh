@@ -78,33 +78,37 @@ __device__ __forceinline__ u64 ld_nc(const u64 *p) {
 #define SBWT_GATHER_EVICT_FIRST 1
 #endif
 
-__device__ __forceinline__ u64 l2_gather_policy(bool evict_first) {
+__device__ __forceinline__ u64 l2_evict_first_policy() {
     u64 p;
-    if (evict_first) asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
-    else asm("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
     return p;
 }
 
-__device__ __forceinline__ uint2 ld_gather_u32x2(const uint2 *p, u64 pol) {
-    uint2 v;
+// A gather: with the evict-first policy pol when ef is set, plainly otherwise.
+__device__ __forceinline__ uint2 ld_gather_u32x2(const uint2 *p, bool ef, u64 pol) {
 #if SBWT_GATHER_EVICT_FIRST
-    asm("ld.global.nc.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;" : "=r"(v.x), "=r"(v.y) : "l"(p), "l"(pol));
-#else
-    (void)pol;
-    v = __ldg(p);
+    if (ef) {
+        uint2 v;
+        asm("ld.global.nc.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;" : "=r"(v.x), "=r"(v.y) : "l"(p), "l"(pol));
+        return v;
+    }
 #endif
-    return v;
+    (void)ef;
+    (void)pol;
+    return __ldg(p);
 }
 
-__device__ __forceinline__ u64 ld_gather_u64(const u64 *p, u64 pol) {
-    u64 v;
+__device__ __forceinline__ u64 ld_gather_u64(const u64 *p, bool ef, u64 pol) {
 #if SBWT_GATHER_EVICT_FIRST
-    asm("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(p), "l"(pol));
-#else
-    (void)pol;
-    v = __ldg(reinterpret_cast<const unsigned long long *>(p));
+    if (ef) {
+        u64 v;
+        asm("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(p), "l"(pol));
+        return v;
+    }
 #endif
-    return v;
+    (void)ef;
+    (void)pol;
+    return __ldg(reinterpret_cast<const unsigned long long *>(p));
 }
 
 // x >> s with the PTX rule that s >= 64 gives 0 (the reference relies on it,

@@ -412,6 +412,7 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
     u32 left = 0;                  // k-mers of the run left of J
     u32 L = 0, Rr = 0, I = kDone;
     u32 V = dev::kNoNode;          // STREAM: node of the k-mer right of J (found), or kNoNode
+    const u64 gpol = l2_evict_first_policy();  // for the gathers from tables too large for L2
 
     for (;;) {
         // ---- fill: new windows once every lane's window is cut, then one run per lane
@@ -476,7 +477,7 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
             if (STREAM && V != dev::kNoNode) {
                 // ---- backward step: k-mer J = x[J] . (first k-1 letters of k-mer J+1)
                 const u32 letter = (u32)(a.words[pos >> 5] >> (62u - 2u * (u32)(pos & 31u))) & 3u;
-                const u32 u = a.sv.back_step(V, letter, l2_gather_policy(a.ef_back));
+                const u32 u = a.sv.back_step(V, letter, a.ef_back, gpol);
                 adv = 1;
                 if (u != dev::kNoNode) found = u;
             } else {
@@ -486,7 +487,7 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
                 const u32 sh = (u32)(b & 63u);
                 kmer = (w0 << sh) | (shr_clamp(w1, 63u - sh) >> 1);
                 if (p) {
-                    const PT e = ld_gather_u32x2(pre + (kmer >> (64u - 2u * p)), l2_gather_policy(a.ef_pre));
+                    const PT e = ld_gather_u32x2(pre + (kmer >> (64u - 2u * p)), a.ef_pre, gpol);
                     L = e.x;
                     Rr = e.y;
                 } else {

@@ -122,15 +122,15 @@ struct StreamView {
     // Node of the k-mer a.y given the node v of the k-mer y.b, or kNoNode: one
     // load of v's entry u0 | group_letters(u0) << 32 (the backward table); the
     // member with first letter a sits after the members with smaller ones.
-    __device__ __forceinline__ u32 back_step(u32 v, u32 a, u64 pol) const {
-        const u64 e = ld_gather_u64(back + v, pol);
+    __device__ __forceinline__ u32 back_step(u32 v, u32 a, bool ef, u64 pol) const {
+        const u64 e = ld_gather_u64(back + v, ef, pol);
         const u32 m = (u32)(e >> 32);
         if (!((m >> (a + 1u)) & 1u)) return kNoNode;
         return (u32)e + (u32)__popc(m & ((1u << (a + 1u)) - 1u));
     }
 #else
     // Node of the k-mer a.y given the node v of the k-mer y.b, or kNoNode.
-    __device__ __forceinline__ u32 back_step(u32 v, u32 a, u64) const {
+    __device__ __forceinline__ u32 back_step(u32 v, u32 a, bool, u64) const {
         u32 u = pred(v);
         if (u >= n) return kNoNode;
         const u32 want = a + 1u;
