@@ -181,7 +181,12 @@ int sbwt_use_graphs(sbwt_index *index, int on);
  * Replaces epic::gpu::launch_search_kernel / search
  * (include/gpu/search_and_presearch_launchers.hpp:21-60,
  *  include/gpu/search_kernel.hpp:61-104).  Unlike the reference, no thread
- * runs past n_kmers. */
+ * runs past n_kmers.  In the run-walking search modes, k-mers at consecutive
+ * positions (each position one more than the one before, as the reference's
+ * positions of one read are) are walked as runs, as sbwt_search_reads does;
+ * the call then waits once on `stream` (the run count sizes the run table),
+ * and positions with runs shorter than four k-mers on average are searched
+ * one k-mer at a time. */
 int sbwt_search_packed(sbwt_index *index, const uint64_t *d_kmer_string, uint64_t n_words,
                        uint64_t *d_positions_in_results_out, uint64_t n_kmers, void *stream);
 

@@ -491,3 +491,27 @@ def test_build_times_reported(small, cuda):
         assert t["lines_ms"] > 0 and t["presearch_ms"] > 0 and t["backward_ms"] > 0 and t["poppy_ms"] == 0
         ix.presearch(12)
         assert ix.build_times()["presearch_ms"] > 0
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("order", ["reads", "shuffled", "mixed"])
+def test_search_packed_runs_and_random_positions(small, cuda, mode, order):
+    """The kernel contract with the reference's positions (runs of consecutive positions,
+    walked as runs), shuffled positions (searched per k-mer) and a mix of both, in every mode."""
+    import torch
+    b, k = small["built"], small["k"]
+    ox = orc.OracleIndex(b.bits, b.n_bits)
+    words = orc.pack(small["letters"])
+    pos = orc.positions(small["rows"], k).copy()
+    rng = np.random.default_rng(17)
+    if order == "shuffled":
+        pos = pos[rng.permutation(pos.size)]
+    elif order == "mixed":  # a shuffled tail after runs, and runs that touch at read ends
+        cut = pos.size * 3 // 4
+        pos[cut:] = pos[cut:][rng.permutation(pos.size - cut)]
+    want = ox.search_positions(words, pos, k, 10)
+    with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=10, search_mode=mode) as ix:
+        d_pos = _t(pos, cuda)
+        ix.search_packed(_t(words, cuda), d_pos)
+        torch.cuda.synchronize()
+        assert np.array_equal(_u64(d_pos), want)
