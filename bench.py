@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--no-prefilter", action="store_true", help="skip the learned-prefilter leg")
     ap.add_argument("--no-autotune", action="store_true", help="skip the autotuned leg")
     ap.add_argument("--no-per-kmer", action="store_true", help="skip the leg that searches every k-mer")
+    ap.add_argument("--no-contract", action="store_true", help="skip the leg on the reference's kernel contract")
     ap.add_argument("--search-mode", choices=["every", "skip", "stream"], default="stream",
                     help="main leg: every k-mer searched (as the reference), absent-run skip, or skip + backward steps")
     ap.add_argument("--pf-queries", type=int, default=200_000_000)
@@ -505,6 +506,37 @@ def main():
                        "search_kernel_ms": statistics.mean(t_ms), "output": "membership bitmap only (no answers)"}
         del d_mem2
 
+    # ---- the reference's kernel contract (sbwt_search_packed): packed letters + the reference's
+    # positions array (k-mer j of read r at row_start[r] + i), answers written over the positions
+    contract = None
+    if rank == 0 and not args.no_contract:
+        lens = torch.from_numpy(np.diff(rows.astype(np.int64))).to(dev)
+        cnt = torch.clamp(lens - (k - 1), min=0)
+        rs = d_rows[:-1]
+        ks = torch.cumsum(cnt, 0) - cnt  # first k-mer index of each row
+        d_pos0 = torch.arange(n_kmers, dtype=torch.int64, device=dev) + torch.repeat_interleave(rs - ks, cnt)
+        n_words = (letters.size + 32 + 31) // 32
+        d_words = torch.empty(n_words, dtype=torch.int64, device=dev)
+        sg._lib.lib.sbwt_pack(sg._ptr(d_letters), letters.size, sg._ptr(d_words), sg._stream_ptr(stream))
+        d_pos = torch.empty_like(d_pos0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c_ms = []
+        for it in range(2 + args.steps):
+            d_pos.copy_(d_pos0)
+            torch.cuda.synchronize(dev)
+            e0.record(stream)
+            ix.search_packed(d_words, d_pos, stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            if it >= 2:
+                c_ms.append(e0.elapsed_time(e1))
+        if not np.array_equal(d_pos[: ans.size].cpu().numpy().view(np.uint64), ans):
+            raise SystemExit("bench: kernel-contract answers differ from the oracle")
+        cm = statistics.mean(c_ms)
+        contract = {"value": n_kmers / (cm / 1e3), "ms_per_call": cm, "entry_point": "sbwt_search_packed",
+                    "note": "positions array in, answers out in place, as the reference's search kernel"}
+        del d_pos, d_pos0, d_words, lens, cnt, rs, ks
+
     # ---- autotuned leg: the tuner picks shape and presearch depth on a sample, then the batch is timed again
     tuned = None
     if not args.no_autotune and rank == 0:
@@ -572,6 +604,7 @@ def main():
             "clocks": clk,
             "per_kmer": per_kmer,
             "membership_only": member_only,
+            "kernel_contract": contract,
             "autotuned": tuned,
             "prefilter": prefilter,
         }
