@@ -18,16 +18,64 @@
 namespace sbwt {
 namespace {
 
-struct RunStart {
-    const u64 *pos;
-    __device__ __forceinline__ bool operator()(const u64 j) const { return j == 0 || pos[j] != pos[j - 1] + 1u; }
-};
+// Run starts are found in two passes over the positions, each thread block
+// taking kBlockItems consecutive k-mers: pass 1 counts the starts of each
+// block, an exclusive scan of the counts gives each block its first output
+// slot, and pass 2 writes the start indices in order (warp ballots, then the
+// warps' counts in shared memory).
+constexpr u32 kThreads = 256;
+constexpr u32 kPerThread = 16;
+constexpr u32 kBlockItems = kThreads * kPerThread;
 
-__global__ void count_runs_kernel(const u64 *__restrict__ pos, u64 n, unsigned long long *__restrict__ count) {
-    const u64 j = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool start = j < n && (j == 0 || pos[j] != pos[j - 1] + 1u);
-    const u32 m = __ballot_sync(0xffffffffu, start);
-    if ((threadIdx.x & 31u) == 0 && m) atomicAdd(count, (unsigned long long)__popc(m));
+__device__ __forceinline__ bool run_start(const u64 *__restrict__ pos, u64 j) {
+    return j == 0 || pos[j] != pos[j - 1] + 1u;
+}
+
+__global__ void __launch_bounds__(kThreads) block_starts_kernel(const u64 *__restrict__ pos, u64 n,
+                                                                u64 *__restrict__ block_count) {
+    __shared__ u32 warp_sum[kThreads / 32];
+    const u64 base = (u64)blockIdx.x * kBlockItems;
+    u32 c = 0;
+#pragma unroll 4
+    for (u32 it = 0; it < kPerThread; it++) {
+        const u64 j = base + it * kThreads + threadIdx.x;
+        c += (j < n && run_start(pos, j)) ? 1u : 0u;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31u) == 0) warp_sum[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        u32 t = 0;
+        for (u32 w = 0; w < kThreads / 32; w++) t += warp_sum[w];
+        block_count[blockIdx.x] = t;
+    }
+}
+
+// kstart[block_offset[b] + i] = index of the i-th run start of block b.
+__global__ void __launch_bounds__(kThreads) write_starts_kernel(const u64 *__restrict__ pos, u64 n,
+                                                                const u64 *__restrict__ block_offset,
+                                                                u64 *__restrict__ kstart) {
+    __shared__ u32 warp_cnt[kThreads / 32];
+    const u64 base = (u64)blockIdx.x * kBlockItems;
+    const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    u64 out = block_offset[blockIdx.x];
+    for (u32 it = 0; it < kPerThread; it++) {
+        const u64 j = base + it * kThreads + threadIdx.x;
+        const bool st = j < n && run_start(pos, j);
+        const u32 m = __ballot_sync(0xffffffffu, st);
+        if (lane == 0) warp_cnt[warp] = __popc(m);
+        __syncthreads();
+        u32 before = 0, total = 0;
+        for (u32 w = 0; w < kThreads / 32; w++) {
+            const u32 cw = warp_cnt[w];
+            before += w < warp ? cw : 0u;
+            total += cw;
+        }
+        if (st) kstart[out + before + __popc(m & ((1u << lane) - 1u))] = j;
+        out += total;
+        __syncthreads();
+    }
 }
 
 // row_start[r] = letter offset of run r's first k-mer; kstart[n_rows] = n.
@@ -46,24 +94,23 @@ __global__ void run_rows_kernel(const u64 *__restrict__ pos, u64 *__restrict__ k
 // (the run count comes back to the host to size the tables).
 int packed_runs(Workspace &w, const u64 *positions, u64 n_kmers, cudaStream_t s, u64 *n_rows) {
     *n_rows = 0;
-    SBWT_TRY(grow(w.counter, w.counter_cap, 1));
-    SBWT_CHECK_CUDA(cudaMemsetAsync(w.counter, 0, sizeof(unsigned long long), s));
-    const unsigned blocks = (unsigned)((n_kmers + 255) / 256);
-    count_runs_kernel<<<blocks, 256, 0, s>>>(positions, n_kmers, w.counter);
+    const u64 nb = (n_kmers + kBlockItems - 1) / kBlockItems;
+    // w.scan: block counts, then their exclusive scan in place, then the scan's scratch
+    size_t tmp_bytes = 0;
+    SBWT_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, w.scan, w.scan, (int64_t)nb + 1, s));
+    SBWT_TRY(grow(w.scan, w.scan_cap, nb + 1 + tmp_bytes / sizeof(u64) + 1));
+    u64 *counts = w.scan, *tmp = w.scan + nb + 1;
+    SBWT_CHECK_CUDA(cudaMemsetAsync(counts + nb, 0, sizeof(u64), s));
+    block_starts_kernel<<<(unsigned)nb, kThreads, 0, s>>>(positions, n_kmers, counts);
     SBWT_CHECK_CUDA(cudaGetLastError());
-    unsigned long long runs = 0;
-    SBWT_CHECK_CUDA(cudaMemcpyAsync(&runs, w.counter, sizeof runs, cudaMemcpyDeviceToHost, s));
+    SBWT_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, counts, counts, (int64_t)nb + 1, s));
+    u64 runs = 0;
+    SBWT_CHECK_CUDA(cudaMemcpyAsync(&runs, counts + nb, sizeof runs, cudaMemcpyDeviceToHost, s));
     SBWT_CHECK_CUDA(cudaStreamSynchronize(s));
     if (runs == 0 || runs * 4 > n_kmers) return 0;
     SBWT_TRY(grow(w.kstart, w.kstart_cap, runs + 1));
     SBWT_TRY(grow(w.rows, w.rows_cap, runs + 1));
-    size_t tmp_bytes = 0;
-    cub::CountingInputIterator<u64> idx(0);
-    SBWT_CHECK_CUDA(cub::DeviceSelect::If(nullptr, tmp_bytes, idx, w.kstart, w.counter, (int64_t)n_kmers,
-                                          RunStart{positions}, s));
-    SBWT_TRY(grow(w.scan, w.scan_cap, tmp_bytes / sizeof(u64) + 1));
-    SBWT_CHECK_CUDA(cub::DeviceSelect::If(w.scan, tmp_bytes, idx, w.kstart, w.counter, (int64_t)n_kmers,
-                                          RunStart{positions}, s));
+    write_starts_kernel<<<(unsigned)nb, kThreads, 0, s>>>(positions, n_kmers, counts, w.kstart);
     run_rows_kernel<<<(unsigned)((runs + 255) / 256), 256, 0, s>>>(positions, w.kstart, runs, n_kmers, w.rows);
     SBWT_CHECK_CUDA(cudaGetLastError());
     *n_rows = runs;
