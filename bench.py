@@ -97,11 +97,11 @@ def workload_of(args, rank):
         return [genome], letters, rows, args.p
     if args.workload == "batched":
         import sbwt_gpu_b200 as sg
-        genome = wl.config1(seed=1235)["genome"]
+        genome = wl.small_workload(seed=1235)["genome"]
         d = tempfile.mkdtemp(prefix="sbwt_batched_")
         paths = []
         total = int(500_000_000 * args.scale)
-        for f, (lt, rw) in enumerate(wl.config3_files(genome, seed=1237 + 100 * rank, total_kmers=total)):
+        for f, (lt, rw) in enumerate(wl.uneven_read_files(genome, seed=1237 + 100 * rank, total_kmers=total)):
             path = os.path.join(d, f"q{f:02d}.fa")
             wl.write_fasta(path, lt, rw)
             paths.append(path)
@@ -623,7 +623,7 @@ def prefilter_leg(args, dev, k):
     import torch
     import sbwt_gpu_b200 as sg
     from sbwt_gpu_b200 import workloads as wl
-    w = wl.config1(seed=1235)
+    w = wl.small_workload(seed=1235)
     built = sg.build_sbwt([w["genome"].tobytes()], k)
     pix = sg.Index.from_bits(built.bits, built.n_bits, k=k, k_presearch=10)
     t = time.perf_counter()

@@ -86,7 +86,7 @@ def mixed_reads(rng, genome, n_pos, n_neg, length, sub_rate):
     return np.ascontiguousarray(reads).reshape(-1), rows
 
 
-def config1(seed=1235, scale=1.0):
+def small_workload(seed=1235, scale=1.0):
     rng = rng_for(seed)
     genome = random_bases(rng, int(1_000_000 * scale))
     n_reads = max(2, int(10_000 * scale))
@@ -94,7 +94,7 @@ def config1(seed=1235, scale=1.0):
     return {"name": "small", "genome": genome, "letters": letters, "row_starts": rows, "k": 31, "p": 10}
 
 
-def config2(seed=1236, scale=1.0, reads_scale=None):
+def large_workload(seed=1236, scale=1.0, reads_scale=None):
     rng = rng_for(seed)
     n = int(100_000_000 * scale)
     genome = random_bases(rng, n, gc=0.41)
@@ -117,7 +117,7 @@ def read_lengths(rng, n):
     return np.clip(ln, 31, 100_000)
 
 
-def config3_files(genome, seed=1237, total_kmers=500_000_000, n_files=64, k=31, pos_frac=0.3, sub=0.02):
+def uneven_read_files(genome, seed=1237, total_kmers=500_000_000, n_files=64, k=31, pos_frac=0.3, sub=0.02):
     """Yields (letters, row_starts) for each of n_files query files until total_kmers k-mers."""
     rng = rng_for(seed)
     per_file = total_kmers // n_files

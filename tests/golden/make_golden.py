@@ -48,18 +48,18 @@ SPECS = {
 }
 
 
-# The configuration-1 workload (1,000,000 bp genome, 10,000 reads of 150 bp,
+# The small workload (1,000,000 bp genome, 10,000 reads of 150 bp,
 # k=31, p=10), regenerated from its seed wherever it is needed; only the
-# SHA-256 of the reference's output is stored (config1.json).
-CONFIG1_SEED = 1235
-CONFIG1_JSON = os.path.join(HERE, "config1.json")
+# SHA-256 of the reference's output is stored (small_workload.json).
+SMALL_SEED = 1235
+SMALL_JSON = os.path.join(HERE, "small_workload.json")
 
 
-def write_config1(d):
-    """Writes the config-1 index files and query FASTA into d; returns (n_bits, letters, rows)."""
+def write_small_workload(d):
+    """Writes the small workload's index files and query FASTA into d; returns (n_bits, letters, rows)."""
     import sbwt_gpu_b200 as sg
     from sbwt_gpu_b200 import workloads as wl
-    w = wl.config1(seed=CONFIG1_SEED)
+    w = wl.small_workload(seed=SMALL_SEED)
     built = sg.build_sbwt([w["genome"].tobytes()], w["k"])
     check_safe(built.n_bits, w["letters"], w["row_starts"], w["k"], w["p"])
     os.makedirs(d, exist_ok=True)
@@ -68,7 +68,7 @@ def write_config1(d):
     return built.n_bits, w["letters"], w["row_starts"]
 
 
-def config1_flags(d):
+def small_workload_flags(d):
     return [f"--file-a={d}/ix.A", f"--file-c={d}/ix.C", f"--file-g={d}/ix.G", f"--file-t={d}/ix.T",
             f"--file-queries={d}/queries.fa", "--k=31", "--k-presearch=10", "--threads-per-block=64"]
 
@@ -123,9 +123,9 @@ def prepare():
 def run(out_dir):
     os.makedirs(out_dir, exist_ok=True)
     env = dict(os.environ, MALLOC_PERTURB_="255")
-    c1 = os.path.join(out_dir, "config1_inputs")
-    write_config1(c1)
-    jobs = [(name, case_flags(name)) for name in SPECS] + [("config1", config1_flags(c1))]
+    c1 = os.path.join(out_dir, "small_workload_inputs")
+    write_small_workload(c1)
+    jobs = [(name, case_flags(name)) for name in SPECS] + [("small_workload", small_workload_flags(c1))]
     for name, flags in jobs:
         with open(os.path.join(out_dir, f"{name}.out"), "wb") as fo, \
                 open(os.path.join(out_dir, f"{name}.err"), "wb") as fe:
@@ -155,14 +155,14 @@ def collect(out_dir):
         meta["reference_sha256"] = hashlib.sha256(data).hexdigest()
         json.dump(meta, open(meta_p, "w"), indent=1)
         print(name, len(data), "bytes")
-    err = open(os.path.join(out_dir, "config1.err"), "rb").read()
+    err = open(os.path.join(out_dir, "small_workload.err"), "rb").read()
     if reference_failed(err):
-        raise SystemExit("config1: the reference reported an error")
-    data = open(os.path.join(out_dir, "config1.out"), "rb").read()
-    json.dump({"seed": CONFIG1_SEED, "bytes": len(data), "lines": data.count(b"\n"),
+        raise SystemExit("small workload: the reference reported an error")
+    data = open(os.path.join(out_dir, "small_workload.out"), "rb").read()
+    json.dump({"seed": SMALL_SEED, "bytes": len(data), "lines": data.count(b"\n"),
                "minus_ones": data.count(b"-1 "), "reference_sha256": hashlib.sha256(data).hexdigest()},
-              open(CONFIG1_JSON, "w"), indent=1)
-    print("config1", len(data), "bytes")
+              open(SMALL_JSON, "w"), indent=1)
+    print("small_workload", len(data), "bytes")
 
 
 if __name__ == "__main__":

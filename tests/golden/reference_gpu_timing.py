@@ -48,7 +48,7 @@ def main():
     n_bits = built.n_bits
     del built, genome
     wl.write_fasta(os.path.join(d, "queries.fa"), letters, rows)
-    flags = make_golden.config1_flags(d)
+    flags = make_golden.small_workload_flags(d)
     flags = [f for f in flags if not f.startswith("--k-presearch")] + ["--k-presearch=12", "--do-not-store-results"]
     env = dict(os.environ, MALLOC_PERTURB_="255")
     r = subprocess.run([make_golden.REF_SEARCH] + flags, capture_output=True, env=env, timeout=3600)

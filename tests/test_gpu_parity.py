@@ -224,9 +224,9 @@ def test_search_reads_host_pinned_and_pageable(small, cuda):
         assert np.array_equal(pa.numpy().view(np.uint64), want)
 
 
-def test_config1_full_workload(cuda, tmp_path):
+def test_small_workload_full(cuda, tmp_path):
     import make_golden
-    n, letters, rows = make_golden.write_config1(str(tmp_path))
+    n, letters, rows = make_golden.write_small_workload(str(tmp_path))
     paths = [str(tmp_path / f"ix.{c}") for c in "ACGT"]
     ox = orc.OracleIndex.from_files(paths)
     want = ox.search_reads(letters, rows, 31, 10)
@@ -235,7 +235,7 @@ def test_config1_full_workload(cuda, tmp_path):
         host = ix.search_reads_host(letters, rows)
     assert np.array_equal(got, want)
     assert np.array_equal(host, want)
-    meta_p = os.path.join(GOLDEN, "config1.json")
+    meta_p = os.path.join(GOLDEN, "small_workload.json")
     if os.path.exists(meta_p):
         text = sg.format_answers(rows, 31, got)
         assert hashlib.sha256(text).hexdigest() == json.load(open(meta_p))["reference_sha256"]

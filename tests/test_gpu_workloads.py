@@ -25,7 +25,7 @@ def test_batched_uneven_files_one_launch(cuda, tmp_path):
     genome = wl.random_bases(rng, 300_000)
     built = sg.build_sbwt([genome.tobytes()], 31)
     paths = []
-    for f, (letters, rows) in enumerate(wl.config3_files(genome, seed=32, total_kmers=3_000_000, n_files=64)):
+    for f, (letters, rows) in enumerate(wl.uneven_read_files(genome, seed=32, total_kmers=3_000_000, n_files=64)):
         p = str(tmp_path / f"q{f:02d}.fa")
         wl.write_fasta(p, letters, rows)
         paths.append(p)

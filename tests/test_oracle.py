@@ -129,13 +129,13 @@ def test_oracle_matches_reference_program_output(case):
     assert orc.format_answers(rows, meta["k"], ans) == ref
 
 
-def test_oracle_matches_reference_program_config1(tmp_path):
-    meta_p = os.path.join(GOLDEN, "config1.json")
+def test_oracle_matches_reference_program_small_workload(tmp_path):
+    meta_p = os.path.join(GOLDEN, "small_workload.json")
     if not os.path.exists(meta_p):
         pytest.skip("fixture not generated yet")
     import make_golden
     meta = json.load(open(meta_p))
-    n, letters, rows = make_golden.write_config1(str(tmp_path))
+    n, letters, rows = make_golden.write_small_workload(str(tmp_path))
     ox = orc.OracleIndex.from_files([str(tmp_path / f"ix.{c}") for c in "ACGT"])
     l2, r2, nk = orc.read_queries(open(tmp_path / "queries.fa", "rb").read(), 31)
     assert np.array_equal(l2, letters) and np.array_equal(r2, rows)
