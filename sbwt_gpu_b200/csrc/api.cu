@@ -561,11 +561,9 @@ extern "C" int sbwt_search_packed(sbwt_index *ix, const uint64_t *d_kmer_string,
     if (runs_form(ix)) {
         // runs of consecutive positions go to the run-walking kernel (packed_runs.cu)
         u64 n_rows = 0;
-        SBWT_TRY(packed_runs(w, d_positions_in_results_out, n_kmers, s, &n_rows));
+        SearchArgs a = base_args(ix, true);
+        SBWT_TRY(packed_runs(w, d_positions_in_results_out, n_kmers, a.chunk, s, &n_rows));
         if (n_rows) {
-            SearchArgs a = base_args(ix, true);
-            SBWT_TRY(grow(w.chunk_row, w.chunk_cap, (n_kmers + a.chunk - 1) / a.chunk));
-            SBWT_TRY(launch_chunk_rows(w.kstart, n_rows, n_kmers, a.chunk, w.chunk_row, s));
             a.words = d_kmer_string;
             a.positions = nullptr;
             a.row_starts = w.rows;

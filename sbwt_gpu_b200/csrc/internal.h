@@ -169,7 +169,7 @@ int build_stream(sbwt_index *ix, cudaStream_t s);
 dev::StreamView stream_view(const sbwt_index *ix);
 
 // packed_runs.cu
-int packed_runs(Workspace &w, const u64 *positions, u64 n_kmers, cudaStream_t s, u64 *n_rows);
+int packed_runs(Workspace &w, const u64 *positions, u64 n_kmers, u32 chunk, cudaStream_t s, u64 *n_rows);
 
 // api.cu
 int search_rows_device(sbwt_index *ix, Workspace &w, const uint8_t *d_letters, u64 n_letters, const u64 *d_rows,

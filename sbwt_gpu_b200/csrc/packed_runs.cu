@@ -18,32 +18,42 @@
 namespace sbwt {
 namespace {
 
-// Run starts are found in two passes over the positions, each thread block
-// taking kBlockItems consecutive k-mers: pass 1 counts the starts of each
-// block, an exclusive scan of the counts gives each block its first output
-// slot, and pass 2 writes the start indices in order (warp ballots, then the
-// warps' counts in shared memory).
+// The positions are read once.  Pass 1 (kThreads x kPerThread consecutive
+// k-mers per block) writes the run-start bitmap (bit j of word j/32 = k-mer j
+// starts a run) and counts each block's starts; an exclusive scan of the
+// counts gives each block its first run index; pass 2 reads only the bitmap
+// (one word per thread, kWords words per block: the same k-mers as pass 1's
+// block) and writes the run table and the chunk-row table.
 constexpr u32 kThreads = 256;
 constexpr u32 kPerThread = 16;
 constexpr u32 kBlockItems = kThreads * kPerThread;
+constexpr u32 kWords = kBlockItems / 32;  // pass 2 threads per block
 
-__device__ __forceinline__ bool run_start(const u64 *__restrict__ pos, u64 j) {
-    return j == 0 || pos[j] != pos[j - 1] + 1u;
-}
-
-__global__ void __launch_bounds__(kThreads) block_starts_kernel(const u64 *__restrict__ pos, u64 n,
-                                                                u64 *__restrict__ block_count) {
+__global__ void __launch_bounds__(kThreads) start_bits_kernel(const u64 *__restrict__ pos, u64 n,
+                                                              uint32_t *__restrict__ bits,
+                                                              u64 *__restrict__ block_count) {
     __shared__ u32 warp_sum[kThreads / 32];
     const u64 base = (u64)blockIdx.x * kBlockItems;
-    u32 c = 0;
-#pragma unroll 4
+    const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    u64 v[kPerThread], before[kPerThread];
+#pragma unroll
     for (u32 it = 0; it < kPerThread; it++) {
         const u64 j = base + it * kThreads + threadIdx.x;
-        c += (j < n && run_start(pos, j)) ? 1u : 0u;
+        v[it] = j < n ? pos[j] : 0ull;
+        before[it] = (lane == 0 && j > 0 && j - 1u < n) ? pos[j - 1u] : 0ull;  // the word's left neighbour
     }
+    u32 c = 0;
 #pragma unroll
-    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    if ((threadIdx.x & 31u) == 0) warp_sum[threadIdx.x >> 5] = c;
+    for (u32 it = 0; it < kPerThread; it++) {
+        const u64 j = base + it * kThreads + threadIdx.x;
+        u64 prev = __shfl_up_sync(0xffffffffu, v[it], 1);
+        if (lane == 0) prev = before[it];
+        const bool st = j < n && (j == 0 || v[it] != prev + 1u);
+        const u32 m = __ballot_sync(0xffffffffu, st);
+        if (lane == 0) bits[j >> 5] = m;  // every word of the block, zero past n
+        c += (u32)__popc(m);
+    }
+    if (lane == 0) warp_sum[warp] = c;
     __syncthreads();
     if (threadIdx.x == 0) {
         u32 t = 0;
@@ -52,56 +62,61 @@ __global__ void __launch_bounds__(kThreads) block_starts_kernel(const u64 *__res
     }
 }
 
-// kstart[block_offset[b] + i] = index of the i-th run start of block b.
-__global__ void __launch_bounds__(kThreads) write_starts_kernel(const u64 *__restrict__ pos, u64 n,
-                                                                const u64 *__restrict__ block_offset,
-                                                                u64 *__restrict__ kstart) {
-    __shared__ u32 warp_cnt[kThreads / 32];
-    const u64 base = (u64)blockIdx.x * kBlockItems;
+// Run r (in order of its first k-mer j): kstart[r] = j, row_start[r] =
+// pos[j]; kstart[n_rows] = n.  chunk_row[c] (chunks of chunk_words * 32
+// k-mers) = the run holding k-mer c * chunk_words * 32 = (runs starting at or
+// before it) - 1.
+__global__ void __launch_bounds__(kWords) run_table_kernel(const u64 *__restrict__ pos, u64 n,
+                                                           const uint32_t *__restrict__ bits,
+                                                           const u64 *__restrict__ block_offset, u64 n_rows,
+                                                           u32 chunk_words, u64 *__restrict__ kstart,
+                                                           u64 *__restrict__ row_start, u32 *__restrict__ chunk_row) {
+    __shared__ u32 warp_tot[kWords / 32];
     const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    u64 out = block_offset[blockIdx.x];
-    for (u32 it = 0; it < kPerThread; it++) {
-        const u64 j = base + it * kThreads + threadIdx.x;
-        const bool st = j < n && run_start(pos, j);
-        const u32 m = __ballot_sync(0xffffffffu, st);
-        if (lane == 0) warp_cnt[warp] = __popc(m);
-        __syncthreads();
-        u32 before = 0, total = 0;
-        for (u32 w = 0; w < kThreads / 32; w++) {
-            const u32 cw = warp_cnt[w];
-            before += w < warp ? cw : 0u;
-            total += cw;
-        }
-        if (st) kstart[out + before + __popc(m & ((1u << lane) - 1u))] = j;
-        out += total;
-        __syncthreads();
+    const u64 w = (u64)blockIdx.x * kWords + threadIdx.x;
+    const u32 m = bits[w];
+    const u32 c = (u32)__popc(m);
+    u32 incl = c;  // inclusive scan over the warp
+#pragma unroll
+    for (u32 o = 1; o < 32u; o <<= 1) {
+        const u32 x = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += x;
     }
-}
-
-// row_start[r] = letter offset of run r's first k-mer; kstart[n_rows] = n.
-__global__ void run_rows_kernel(const u64 *__restrict__ pos, u64 *__restrict__ kstart, u64 n_rows, u64 n,
-                                u64 *__restrict__ row_start) {
-    const u64 r = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (r < n_rows) row_start[r] = pos[kstart[r]];
-    if (r == 0) kstart[n_rows] = n;
+    if (lane == 31u) warp_tot[warp] = incl;
+    __syncthreads();
+    u64 out = block_offset[blockIdx.x] + (incl - c);
+    for (u32 q = 0; q < warp; q++) out += warp_tot[q];
+    const u64 j0 = w * 32u;
+    if (j0 < n && w % chunk_words == 0) chunk_row[w / chunk_words] = (u32)(out + (m & 1u) - 1u);
+    for (u32 b = m; b; b &= b - 1u) {
+        const u64 j = j0 + (u32)(__ffs(b) - 1);
+        kstart[out] = j;
+        row_start[out] = pos[j];
+        out++;
+    }
+    if (w == 0) kstart[n_rows] = n;
 }
 
 }  // namespace
 
-// Builds the run table of `positions` into w.kstart (n_rows + 1 entries) and
-// w.rows (n_rows row starts); *n_rows = 0 when the runs average fewer than
-// four k-mers (the caller then searches every k-mer).  Synchronises s once
-// (the run count comes back to the host to size the tables).
-int packed_runs(Workspace &w, const u64 *positions, u64 n_kmers, cudaStream_t s, u64 *n_rows) {
+// Builds the run table of `positions` into w.kstart (n_rows + 1 entries),
+// w.rows (n_rows row starts) and w.chunk_row (the run of every chunk-th
+// k-mer; chunk a multiple of 32); *n_rows = 0 when the runs average fewer
+// than four k-mers (the caller then searches every k-mer).  Synchronises s
+// once (the run count comes back to the host to size the tables).
+int packed_runs(Workspace &w, const u64 *positions, u64 n_kmers, u32 chunk, cudaStream_t s, u64 *n_rows) {
     *n_rows = 0;
+    if (chunk == 0 || chunk % 32u) return set_error("run chunks must be whole bitmap words");
     const u64 nb = (n_kmers + kBlockItems - 1) / kBlockItems;
-    // w.scan: block counts, then their exclusive scan in place, then the scan's scratch
+    // w.scan: block counts (then their exclusive scan, in place), the scan's scratch, the start bitmap
     size_t tmp_bytes = 0;
     SBWT_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, w.scan, w.scan, (int64_t)nb + 1, s));
-    SBWT_TRY(grow(w.scan, w.scan_cap, nb + 1 + tmp_bytes / sizeof(u64) + 1));
+    const u64 tmp_words = tmp_bytes / sizeof(u64) + 1;
+    SBWT_TRY(grow(w.scan, w.scan_cap, nb + 1 + tmp_words + nb * (kWords / 2)));
     u64 *counts = w.scan, *tmp = w.scan + nb + 1;
+    uint32_t *bits = reinterpret_cast<uint32_t *>(tmp + tmp_words);
     SBWT_CHECK_CUDA(cudaMemsetAsync(counts + nb, 0, sizeof(u64), s));
-    block_starts_kernel<<<(unsigned)nb, kThreads, 0, s>>>(positions, n_kmers, counts);
+    start_bits_kernel<<<(unsigned)nb, kThreads, 0, s>>>(positions, n_kmers, bits, counts);
     SBWT_CHECK_CUDA(cudaGetLastError());
     SBWT_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, counts, counts, (int64_t)nb + 1, s));
     u64 runs = 0;
@@ -110,8 +125,9 @@ int packed_runs(Workspace &w, const u64 *positions, u64 n_kmers, cudaStream_t s,
     if (runs == 0 || runs * 4 > n_kmers) return 0;
     SBWT_TRY(grow(w.kstart, w.kstart_cap, runs + 1));
     SBWT_TRY(grow(w.rows, w.rows_cap, runs + 1));
-    write_starts_kernel<<<(unsigned)nb, kThreads, 0, s>>>(positions, n_kmers, counts, w.kstart);
-    run_rows_kernel<<<(unsigned)((runs + 255) / 256), 256, 0, s>>>(positions, w.kstart, runs, n_kmers, w.rows);
+    SBWT_TRY(grow(w.chunk_row, w.chunk_cap, (n_kmers + chunk - 1) / chunk));
+    run_table_kernel<<<(unsigned)nb, kWords, 0, s>>>(positions, n_kmers, bits, counts, runs, chunk / 32u, w.kstart,
+                                                     w.rows, w.chunk_row);
     SBWT_CHECK_CUDA(cudaGetLastError());
     *n_rows = runs;
     return 0;
