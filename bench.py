@@ -12,8 +12,10 @@ One step = one pass of the search path over the whole batch:
            timed with CUDA events on the launching stream (inputs and outputs,
            1.5 GB + 9.6 GB, are larger than L2; no flush needed);
   `e2e`:   the same through sbwt_search_reads_host with pinned host buffers:
-           letters and row starts host->device, answers device->host, inside
-           the timed region (host wall clock around the synchronous call).
+           letters and row starts host->device, answers device->host (as a
+           bitmap + the found k-mers' node ids, expanded into the u64 answers
+           by the host threads), inside the timed region (host wall clock
+           around the synchronous call).
 With --gpus N (torchrun), every rank holds a replica of the index and searches
 its own 10M reads (weak scaling, no collective on the data path); the time
 is the max over ranks.
@@ -432,10 +434,25 @@ def main():
             e2e_s = max_over_ranks(e2e_s)
         if rank == 0 and not np.array_equal(h_ans[: ans.size].numpy().view(np.uint64), ans):
             raise SystemExit("bench: end-to-end answers differ from the oracle")
-        e2e = {"value": n_kmers * world * args.e2e_steps / e2e_s, "unit": UNIT,
-               "h2d_bytes_per_step": int(letters.nbytes + rows.nbytes), "d2h_bytes_per_step": int(n_kmers * 8)}
-        # membership only (sbwt_search_reads_host_member): the bitmap crosses the bus, not the answers
+        d_back = h_ans.to(dev)  # every answer against the device search's (checked against the oracle above)
+        if not torch.equal(d_back, d_ans):
+            raise SystemExit("bench: end-to-end answers differ from the device search's")
+        found = int((d_ans != -1).sum().item())
+        del d_back
+        # the answers cross PCIe in sparse form (bitmap, group offsets, 32-bit node ids of the found
+        # k-mers) while the index has fewer than 2^32 columns and six or more host threads expand them
+        omp_env = os.environ.get("OMP_NUM_THREADS", "").split(",")[0].strip()
+        omp_threads = int(omp_env) if omp_env.isdigit() else len(os.sched_getaffinity(0))
+        mode = os.environ.get("SBWT_PIPELINE_TRANSFER", "")
+        sparse = info["n_bits"] <= 0xFFFFFFFF and (mode == "sparse" or (mode != "dense" and omp_threads >= 6))
         n_words = (n_kmers + 31) // 32
+        d2h = n_words * 4 + ((n_words + 63) // 64 + 1) * 8 + found * 4 if sparse else n_kmers * 8
+        e2e = {"value": n_kmers * world * args.e2e_steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(letters.nbytes + rows.nbytes), "d2h_bytes_per_step": int(d2h),
+               "answer_bytes_per_step": int(n_kmers * 8),
+               "transfer": ("sparse: membership bitmap + group offsets + found node ids (32 bits), expanded "
+                            "into the u64 answers by the host threads") if sparse else "u64 answers"}
+        # membership only (sbwt_search_reads_host_member): the bitmap crosses the bus, not the answers
         h_mem = torch.empty(n_words, dtype=torch.int32).pin_memory()
         ix.member_reads_host(h_letters, h_rows, h_mem)  # warm-up
         if world > 1:

@@ -17,8 +17,10 @@ namespace sbwt {
 
 void Workspace::release() {
     cudaFree(words); cudaFree(kstart); cudaFree(chunk_row); cudaFree(scan); cudaFree(counter);
-    cudaFree(letters); cudaFree(rows); cudaFree(answers); cudaFree(member);
+    cudaFree(letters); cudaFree(rows); cudaFree(answers); cudaFree(member); cudaFree(goff); cudaFree(nodes);
     if (h_rows) cudaFreeHost(h_rows);
+    if (h_goff) cudaFreeHost(h_goff);
+    if (h_nodes) cudaFreeHost(h_nodes);
     if (h_member) cudaFreeHost(h_member);
     if (h_letters) cudaFreeHost(h_letters);
     if (h_answers) cudaFreeHost(h_answers);

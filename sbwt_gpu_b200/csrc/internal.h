@@ -81,8 +81,14 @@ struct Workspace {
     uint64_t *h_rows = nullptr; size_t h_rows_cap = 0;  // pinned host staging
     uint8_t *h_letters = nullptr; size_t h_letters_cap = 0;
     uint64_t *h_answers = nullptr; size_t h_answers_cap = 0;
-    uint32_t *member = nullptr; size_t member_cap = 0;    // membership-only pipeline
+    uint32_t *member = nullptr; size_t member_cap = 0;    // membership bitmap (both host pipelines)
     uint32_t *h_member = nullptr; size_t h_member_cap = 0;
+    // sparse answers of the host pipeline: per group of k-mers the offset of
+    // its first found node id, and the found node ids (32 bits) in order
+    uint64_t *goff = nullptr;   size_t goff_cap = 0;     // group offsets, then the scan's scratch
+    uint32_t *nodes = nullptr;  size_t nodes_cap = 0;
+    uint64_t *h_goff = nullptr; size_t h_goff_cap = 0;
+    uint32_t *h_nodes = nullptr; size_t h_nodes_cap = 0;
     // CUDA graph of the last pack -> table -> search -> bitmap chain, replayed
     // while every launch parameter (the key) stays the same
     cudaGraphExec_t graph = nullptr;

@@ -5,18 +5,41 @@
 // copies of one chunk overlap the search of another while the host prepares
 // the next.
 //
+// The u64 answers do not cross PCIe as such (8 bytes a k-mer would make the
+// device->host copy the bound): while node ids fit in 32 bits and at least
+// six host threads can expand them, a chunk comes back as its membership
+// bitmap, per-group offsets and the found node ids, and the host threads
+// expand them into the caller's answers.  Per chunk b
+// the loop issues b, starts the node-id copy of b-1 (its count is known once
+// b-1's bitmap and offsets are in) and expands b-2.
+//
 // This replaces the strictly sequential host<->device chain of the reference
 // (KmerSearch::search, include/epicseq/kmer_search.hpp:97-160: one H2D of the
 // whole query, pack, positions, search, then one D2H of all results in
 // ResultsPersister::save_results_to_file, results_persister.hpp:58-65).
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
+#if defined(__x86_64__)
+#include <emmintrin.h>
+#endif
+
+#include <cub/cub.cuh>
+#include <omp.h>
 
 #include "internal.h"
 
 namespace sbwt {
 namespace {
+
+#if defined(__x86_64__)
+inline void store_stream(u64 *p, u64 v) { _mm_stream_si64(reinterpret_cast<long long *>(p), (long long)v); }
+inline void store_fence() { _mm_sfence(); }
+#else
+inline void store_stream(u64 *p, u64 v) { *p = v; }
+inline void store_fence() {}
+#endif
 
 bool is_pinned(const void *p) {
     cudaPointerAttributes at;
@@ -34,8 +57,116 @@ struct Chunk {
 };
 
 // Letters per chunk: large enough to amortise the launches, small enough
-// that two chunks in flight stay well inside device memory.
+// that two chunks in flight stay well inside device memory.  The
+// environment variable SBWT_PIPELINE_CHUNK_LETTERS (at least 4096) sets
+// another size.
 constexpr u64 kChunkLetters = 64ull << 20;
+
+u64 chunk_letters() {
+    const char *e = std::getenv("SBWT_PIPELINE_CHUNK_LETTERS");
+    if (!e || !*e) return kChunkLetters;
+    const unsigned long long v = std::strtoull(e, nullptr, 10);
+    return v >= 4096 ? (u64)v : kChunkLetters;
+}
+
+// Sparse answers.  A chunk's answers leave the device as its membership
+// bitmap, the offset of every group of kGroupWords bitmap words (2048
+// k-mers) into the list of found node ids, and that list (32 bits a node):
+// 0.125 + 4 x (found fraction) bytes per k-mer instead of 8.  The host
+// expands them into the u64 answers (~0 for an absent k-mer).
+constexpr u32 kGroupWords = 64;
+constexpr int kMinExpandThreads = 6;
+
+// The environment variable SBWT_PIPELINE_TRANSFER = "dense" or "sparse"
+// overrides the choice by thread count.
+bool sparse_transfer() {
+    const char *e = std::getenv("SBWT_PIPELINE_TRANSFER");
+    if (e && std::strcmp(e, "dense") == 0) return false;
+    if (e && std::strcmp(e, "sparse") == 0) return true;
+    return omp_get_max_threads() >= kMinExpandThreads;
+}
+constexpr u32 kGroupWarps = 4;  // groups (warps) per block of group_nodes_kernel
+
+// gcnt[g] = found k-mers of group g; gcnt[ng] = 0 (the exclusive scan's total).
+__global__ void group_count_kernel(const uint32_t *__restrict__ member, u64 nw, u64 ng, u64 *__restrict__ gcnt) {
+    const u64 g = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const u32 lane = threadIdx.x & 31u;
+    if (g > ng) return;  // whole warps
+    u32 c = 0;
+    if (g < ng) {
+        for (u32 h = 0; h < kGroupWords; h += 32u) {
+            const u64 w = g * kGroupWords + h + lane;
+            if (w < nw) c += (u32)__popc(member[w]);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) gcnt[g] = c;
+}
+
+// nodes[goff[g] + i] = node id of the i-th found k-mer of group g.  One warp
+// per group gathers them into shared memory, then stores them in order
+// (coalesced).
+__global__ void __launch_bounds__(32 * kGroupWarps) group_nodes_kernel(const uint32_t *__restrict__ member,
+                                                                       const u64 *__restrict__ answers, u64 nw,
+                                                                       u64 ng, const u64 *__restrict__ goff,
+                                                                       uint32_t *__restrict__ nodes) {
+    __shared__ uint32_t buf[kGroupWarps][kGroupWords * 32];
+    const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const u64 g = (u64)blockIdx.x * kGroupWarps + warp;
+    if (g >= ng) return;  // whole warps
+    uint32_t *b = buf[warp];
+    u32 o = 0;
+    for (u32 h = 0; h < kGroupWords; h += 32u) {
+        const u64 w = g * kGroupWords + h + lane;
+        const u32 m = w < nw ? member[w] : 0u;
+        const u32 c = (u32)__popc(m);
+        u32 incl = c;
+#pragma unroll
+        for (u32 d = 1; d < 32u; d <<= 1) {
+            const u32 x = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += x;
+        }
+        u32 q = o + incl - c;
+        for (u32 r = m; r; r &= r - 1u) b[q++] = (uint32_t)answers[w * 32u + (u32)(__ffs(r) - 1)];
+        o += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    __syncwarp();
+    uint32_t *dst = nodes + goff[g];
+    for (u32 q = lane; q < o; q += 32u) dst[q] = b[q];
+}
+
+// answers[j] for the nk k-mers of one chunk from its sparse form (streaming
+// stores: the answers are not read back by this thread).
+void expand_answers(u64 *answers, u64 nk, const uint32_t *member, const u64 *goff, const uint32_t *nodes) {
+    const u64 nw = (nk + 31) / 32, ng = (nw + kGroupWords - 1) / kGroupWords;
+#pragma omp parallel if (nk > (1u << 16))
+    {
+#pragma omp for schedule(static)
+        for (int64_t g = 0; g < (int64_t)ng; g++) {
+            u64 o = goff[g];
+            const u64 w1 = std::min<u64>((u64)(g + 1) * kGroupWords, nw);
+            for (u64 w = (u64)g * kGroupWords; w < w1; w++) {
+                const uint32_t m = member[w];
+                u64 *dst = answers + w * 32u;
+                const u32 lim = (u32)std::min<u64>(32u, nk - w * 32u);
+                if (lim == 32u && m == 0u) {
+                    for (u32 i = 0; i < 32u; i++) store_stream(dst + i, ~0ull);
+                } else if (lim == 32u && m == ~0u) {
+                    for (u32 i = 0; i < 32u; i++) store_stream(dst + i, (u64)nodes[o + i]);
+                    o += 32u;
+                } else {
+                    for (u32 i = 0; i < lim; i++) {
+                        const u32 bit = (m >> i) & 1u;
+                        store_stream(dst + i, bit ? (u64)nodes[o] : ~0ull);
+                        o += bit;
+                    }
+                }
+            }
+        }
+        store_fence();
+    }
+}
 
 }  // namespace
 }  // namespace sbwt
@@ -71,11 +202,12 @@ int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, con
     // chunks of whole rows: the end of each is found by binary search in the sorted row starts
     std::vector<Chunk> chunks;
     {
+        const u64 chunk_size = chunk_letters();
         u64 r0 = 0, k0 = 0;
         while (r0 < n_rows) {
             const u64 *first = row_starts + r0 + 1, *last = row_starts + n_rows + 1;
-            // first row end at or past kChunkLetters letters; at least one row per chunk
-            u64 r1 = (u64)(std::lower_bound(first, last, row_starts[r0] + kChunkLetters) - row_starts);
+            // first row end at or past chunk_size letters; at least one row per chunk
+            u64 r1 = (u64)(std::lower_bound(first, last, row_starts[r0] + chunk_size) - row_starts);
             r1 = std::min<u64>(std::max<u64>(r1, r0 + 1), n_rows);
             u64 nk = 0;
 #pragma omp parallel for schedule(static) reduction(+ : nk) if (r1 - r0 > (1u << 16))
@@ -93,7 +225,11 @@ int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, con
     for (int i = 0; i < kSlots; i++)
         if (!ix->pipe_stream[i]) SBWT_CHECK_CUDA(cudaStreamCreateWithFlags(&ix->pipe_stream[i], cudaStreamNonBlocking));
     const bool pin_in = is_pinned(letters);
-    const bool pin_out = answers && (n_kmers == 0 || is_pinned(answers));
+    // answers leave the device in sparse form while node ids fit in 32 bits
+    // and enough host threads expand them faster than PCIe brings u64
+    // answers (about 11 GB/s of answers per thread against 57 GB/s)
+    const bool sparse = answers && ix->n <= 0xffffffffull && sparse_transfer();
+    const bool pin_out = answers && !sparse && (n_kmers == 0 || is_pinned(answers));
     u64 max_letters = 0, max_rows = 0, max_k = 0;
     for (const Chunk &c : chunks) {
         max_letters = std::max(max_letters, c.l1 - c.l0);
@@ -101,33 +237,72 @@ int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, con
         max_k = std::max(max_k, c.nk);
     }
     const u64 max_words = (max_k + 31) / 32;
+    const u64 max_groups = (max_words + kGroupWords - 1) / kGroupWords;
+    size_t scan_bytes = 0;  // scratch of the group-offset scan (w.goff after the offsets)
+    if (sparse)
+        SBWT_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (u64 *)nullptr, (u64 *)nullptr,
+                                                      (int64_t)max_groups + 1));
+    const u64 scan_words = scan_bytes / sizeof(u64) + 1;
     for (int i = 0; i < kSlots; i++) {
         Workspace &w = ix->ws[i];
         SBWT_TRY(grow(w.letters, w.letters_cap, max_letters + 16));
         SBWT_TRY(grow(w.rows, w.rows_cap, max_rows + 1));
         SBWT_TRY(grow_host(w.h_rows, w.h_rows_cap, max_rows + 1));
         if (!pin_in) SBWT_TRY(grow_host(w.h_letters, w.h_letters_cap, max_letters + 16));
-        if (answers) {
-            SBWT_TRY(grow(w.answers, w.answers_cap, max_k));
+        if (answers) SBWT_TRY(grow(w.answers, w.answers_cap, max_k));
+        if (answers && !sparse) {
             if (!pin_out) SBWT_TRY(grow_host(w.h_answers, w.h_answers_cap, max_k));
         } else {
             SBWT_TRY(grow(w.member, w.member_cap, max_words + 1));
             SBWT_TRY(grow_host(w.h_member, w.h_member_cap, max_words + 1));
         }
+        if (sparse) {
+            SBWT_TRY(grow(w.goff, w.goff_cap, max_groups + 1 + scan_words));
+            SBWT_TRY(grow(w.nodes, w.nodes_cap, max_k));
+            SBWT_TRY(grow_host(w.h_goff, w.h_goff_cap, max_groups + 1));
+            SBWT_TRY(grow_host(w.h_nodes, w.h_nodes_cap, max_k));
+        }
     }
     if (member) std::memset(member, 0, (n_kmers + 31) / 32 * sizeof(uint32_t));
-    // pending[i]: chunk whose results sit in slot i's pinned staging
+    // pending[i]: chunk whose results sit in slot i's pinned staging (or are
+    // on their way there); stage[i]: 0 idle, 1 issued, 2 (sparse) node ids
+    // requested
     long pending[kSlots];
-    for (long &x : pending) x = -1;
-    auto drain = [&](int slot) -> int {
+    int stage[kSlots];
+    for (int i = 0; i < kSlots; i++) pending[i] = -1, stage[i] = 0;
+    // sparse: once the slot's bitmap and group offsets are in, the number of
+    // node ids is known and their copy can start
+    auto fetch_nodes = [&](int slot) -> int {
+        if (!sparse || stage[slot] != 1) return 0;
+        stage[slot] = 2;
+        if (pending[slot] < 0) return 0;
         SBWT_CHECK_CUDA(cudaStreamSynchronize(ix->pipe_stream[slot]));
+        const Chunk &c = chunks[(size_t)pending[slot]];
+        Workspace &w = ix->ws[slot];
+        const u64 ng = ((c.nk + 31) / 32 + kGroupWords - 1) / kGroupWords;
+        const u64 found = w.h_goff[ng];
+        if (found > c.nk)
+            return set_error("sparse answers: %llu node ids for %llu k-mers", (unsigned long long)found,
+                             (unsigned long long)c.nk);
+        if (found)
+            SBWT_CHECK_CUDA(cudaMemcpyAsync(w.h_nodes, w.nodes, found * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                            ix->pipe_stream[slot]));
+        return 0;
+    };
+    auto drain = [&](int slot) -> int {
+        SBWT_TRY(fetch_nodes(slot));
+        SBWT_CHECK_CUDA(cudaStreamSynchronize(ix->pipe_stream[slot]));
+        stage[slot] = 0;
         if (pending[slot] >= 0) {
             const Chunk &c = chunks[(size_t)pending[slot]];
-            if (answers) {
-                std::memcpy(answers + c.k0, ix->ws[slot].h_answers, c.nk * sizeof(u64));
+            Workspace &w = ix->ws[slot];
+            if (sparse) {
+                expand_answers(answers + c.k0, c.nk, w.h_member, w.h_goff, w.h_nodes);
+            } else if (answers) {
+                std::memcpy(answers + c.k0, w.h_answers, c.nk * sizeof(u64));
             } else {
                 // the chunk's bitmap starts at bit k0 of the output: shift it into place
-                const uint32_t *src = ix->ws[slot].h_member;
+                const uint32_t *src = w.h_member;
                 const u64 nw = (c.nk + 31) / 32, w0 = c.k0 >> 5;
                 const u32 sh = (u32)(c.k0 & 31u);
                 const u64 out_words = (n_kmers + 31) / 32;
@@ -163,7 +338,31 @@ int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, con
             std::memcpy(w.h_letters, letters + c.l0, nl);
             SBWT_CHECK_CUDA(cudaMemcpyAsync(w.letters, w.h_letters, nl, cudaMemcpyHostToDevice, s));
         }
-        if (answers) {
+        stage[slot] = 1;
+        if (sparse) {
+            // answers and bitmap in one search, then the found node ids gathered per group
+            SBWT_TRY(search_rows_device(ix, w, w.letters, nl, w.rows, nr, w.answers, w.member, c.nk, s));
+            if (c.nk) {
+                const u64 nw = (c.nk + 31) / 32, ng = (nw + kGroupWords - 1) / kGroupWords;
+                u64 *goff = w.goff;
+                void *tmp = w.goff + max_groups + 1;
+                size_t tb = 0;
+                SBWT_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, goff, goff, (int64_t)ng + 1, s));
+                if (tb > scan_words * sizeof(u64)) return set_error("sparse answers: scan scratch too small");
+                group_count_kernel<<<(unsigned)(((ng + 1) * 32 + 255) / 256), 256, 0, s>>>(w.member, nw, ng, goff);
+                SBWT_CHECK_CUDA(cudaGetLastError());
+                SBWT_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, goff, goff, (int64_t)ng + 1, s));
+                group_nodes_kernel<<<(unsigned)((ng + kGroupWarps - 1) / kGroupWarps), 32 * kGroupWarps, 0, s>>>(
+                    w.member, w.answers, nw, ng, goff, w.nodes);
+                SBWT_CHECK_CUDA(cudaGetLastError());
+                SBWT_CHECK_CUDA(cudaMemcpyAsync(w.h_member, w.member, nw * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+                SBWT_CHECK_CUDA(cudaMemcpyAsync(w.h_goff, goff, (ng + 1) * sizeof(u64), cudaMemcpyDeviceToHost, s));
+                pending[slot] = (long)b;
+            }
+            // the previous chunk's node ids start on their way; the one before is expanded
+            if (b >= 1) SBWT_TRY(fetch_nodes((int)((b - 1) % kSlots)));
+            if (b >= 2) SBWT_TRY(drain((int)((b - 2) % kSlots)));
+        } else if (answers) {
             SBWT_TRY(search_rows_device(ix, w, w.letters, nl, w.rows, nr, w.answers, nullptr, c.nk, s));
             if (c.nk) {
                 if (pin_out) {
@@ -182,6 +381,7 @@ int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, con
             pending[slot] = (long)b;
         }
     }
+    // the chunks still in flight, oldest first
     for (size_t i = 0; i < (size_t)kSlots; i++) SBWT_TRY(drain((int)((chunks.size() + i) % kSlots)));
     return 0;
 }

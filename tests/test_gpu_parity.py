@@ -484,6 +484,46 @@ def test_host_pipelines_across_chunks(small, cuda):
     assert np.array_equal(mem, _bits_of(want))
 
 
+@pytest.mark.parametrize("transfer", ["sparse", "dense"])
+@pytest.mark.parametrize("chunk", [4096, 50_000])
+def test_host_answers_sparse_transfer_many_chunks(small, cuda, monkeypatch, chunk, transfer):
+    """The host answers pipeline brings a chunk's answers back as its membership bitmap, group
+    offsets and found node ids and expands them on the host (or, dense, as u64 answers).  Many
+    chunks (every stage of the three-slot rotation), chunks where every k-mer is found (genome
+    reads only), reads without a found k-mer, ragged, empty and shorter-than-k rows, against the
+    oracle."""
+    b, k = small["built"], small["k"]
+    rng = wl.rng_for(91)
+    g = small["genome"]
+    parts = []
+    for i in range(400):
+        length = int(rng.integers(0, 400))
+        if i % 4 == 0:  # genome substring: every k-mer found
+            s0 = int(rng.integers(0, g.size - 400))
+            parts.append(g[s0:s0 + length])
+        elif i % 4 == 1:
+            parts.append(wl.uniform_reads(rng, 1, length).reshape(-1))
+        elif i % 4 == 2:
+            parts.append(np.zeros(0, np.uint8))
+        else:  # at most one k-mer
+            s0 = int(rng.integers(0, g.size - 400))
+            parts.append(g[s0:s0 + int(rng.integers(0, k + 1))])
+    parts += [g[i * 3000:(i + 1) * 3000] for i in range(20)]  # whole chunks of found k-mers
+    letters = np.ascontiguousarray(np.concatenate(parts).astype(np.uint8))
+    rows = np.zeros(len(parts) + 1, dtype=np.uint64)
+    rows[1:] = np.cumsum([p.size for p in parts])
+    want = orc.OracleIndex(b.bits, b.n_bits).search_reads(letters, rows, k, 10)
+    monkeypatch.setenv("SBWT_PIPELINE_CHUNK_LETTERS", str(chunk))
+    monkeypatch.setenv("SBWT_PIPELINE_TRANSFER", transfer)
+    with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=10) as ix:
+        host = ix.search_reads_host(letters, rows)
+        mem = ix.member_reads_host(letters, rows)
+    assert letters.size > 2 * chunk
+    assert (want != orc.NOT_FOUND).mean() > 0.3 and (want == orc.NOT_FOUND).any()
+    assert np.array_equal(host, want)
+    assert np.array_equal(mem, _bits_of(want))
+
+
 def test_build_times_reported(small, cuda):
     b = small["built"]
     with sg.Index.from_bits(b.bits, b.n_bits, k=31, k_presearch=10) as ix:
