@@ -228,7 +228,13 @@ int sbwt_search_reads_noalloc(sbwt_index *index, const uint8_t *d_letters, uint6
 
 /* Host-memory form of sbwt_search_reads: letters, row starts and answers
  * are host buffers (pinned or pageable).  The batch is streamed through the
- * GPU in chunks with copies overlapped with compute.  Replaces the
+ * GPU in chunks with copies overlapped with compute.  While the index has
+ * fewer than 2^32 columns and six or more OpenMP threads are available, the
+ * answers cross PCIe as a membership bitmap plus the 32-bit node ids of the
+ * found k-mers, and the host threads write the u64 answers; environment:
+ * SBWT_PIPELINE_TRANSFER=dense|sparse forces one form,
+ * SBWT_PIPELINE_CHUNK_LETTERS sets the chunk size (default 64M letters).
+ * Replaces the
  * parse/position/search/copy-back chain of KmerSearch::search
  * (kmer_search.hpp:97-160) and ResultsPersister's device-to-host copy
  * (results_persister.hpp:58-65). */
