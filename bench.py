@@ -437,22 +437,20 @@ def main():
         d_back = h_ans.to(dev)  # every answer against the device search's (checked against the oracle above)
         if not torch.equal(d_back, d_ans):
             raise SystemExit("bench: end-to-end answers differ from the device search's")
-        found = int((d_ans != -1).sum().item())
-        del d_back
-        # the answers cross PCIe in sparse form (bitmap, group offsets, 32-bit node ids of the found
-        # k-mers) while the index has fewer than 2^32 columns and six or more host threads expand them
-        omp_env = os.environ.get("OMP_NUM_THREADS", "").split(",")[0].strip()
-        omp_threads = int(omp_env) if omp_env.isdigit() else len(os.sched_getaffinity(0))
-        mode = os.environ.get("SBWT_PIPELINE_TRANSFER", "")
-        sparse = info["n_bits"] <= 0xFFFFFFFF and (mode == "sparse" or (mode != "dense" and omp_threads >= 6))
-        n_words = (n_kmers + 31) // 32
-        d2h = n_words * 4 + ((n_words + 63) // 64 + 1) * 8 + found * 4 if sparse else n_kmers * 8
+        # bytes that crossed PCIe in the last call: the answers come back as bitmap + group offsets +
+        # 32-bit node ids of the found k-mers (sparse, expanded by the host threads), as u64 answers
+        # (dense), or both (hybrid; SBWT_PIPELINE_TRANSFER picks one, else by host thread count)
+        moved = ix.pipeline_bytes()
+        mode = os.environ.get("SBWT_PIPELINE_TRANSFER", "") or "auto"
         e2e = {"value": n_kmers * world * args.e2e_steps / e2e_s, "unit": UNIT,
-               "h2d_bytes_per_step": int(letters.nbytes + rows.nbytes), "d2h_bytes_per_step": int(d2h),
+               "h2d_bytes_per_step": int(moved["h2d"]), "d2h_bytes_per_step": int(moved["d2h"]),
                "answer_bytes_per_step": int(n_kmers * 8),
-               "transfer": ("sparse: membership bitmap + group offsets + found node ids (32 bits), expanded "
-                            "into the u64 answers by the host threads") if sparse else "u64 answers"}
+               "transfer": mode + (": u64 answers" if moved["d2h"] >= n_kmers * 8 else
+                                   ": every fourth chunk as u64 answers, the others as bitmap + found node ids"
+                                   if mode == "hybrid" else
+                                   ": bitmap + found node ids, expanded into the u64 answers by the host threads")}
         # membership only (sbwt_search_reads_host_member): the bitmap crosses the bus, not the answers
+        n_words = (n_kmers + 31) // 32
         h_mem = torch.empty(n_words, dtype=torch.int32).pin_memory()
         ix.member_reads_host(h_letters, h_rows, h_mem)  # warm-up
         if world > 1:
@@ -468,9 +466,10 @@ def main():
             want_bits = bits_of(ans)[:full]
             if not np.array_equal(h_mem[:full].numpy().view(np.uint32), want_bits):
                 raise SystemExit("bench: end-to-end membership bits differ from the oracle")
+        moved = ix.pipeline_bytes()
         e2e["membership_only"] = {"value": n_kmers * world * args.e2e_steps / m_s, "unit": UNIT,
-                                  "h2d_bytes_per_step": int(letters.nbytes + rows.nbytes),
-                                  "d2h_bytes_per_step": int(n_words * 4),
+                                  "h2d_bytes_per_step": int(moved["h2d"]),
+                                  "d2h_bytes_per_step": int(moved["d2h"]),
                                   "entry_point": "sbwt_search_reads_host_member"}
 
     # ---- the same batch with every k-mer searched (the reference's per-k-mer work), for comparison

@@ -241,6 +241,12 @@ int sbwt_search_reads_noalloc(sbwt_index *index, const uint8_t *d_letters, uint6
 int sbwt_search_reads_host(sbwt_index *index, const uint8_t *letters, uint64_t n_letters, const uint64_t *row_starts,
                            uint64_t n_rows, uint64_t *answers, uint64_t n_kmers);
 
+/* Bytes the last sbwt_search_reads_host or sbwt_search_reads_host_member
+ * call on this index copied host->device (letters, row tables) and
+ * device->host (answers in the form that crossed PCIe).  No reference
+ * counterpart. */
+int sbwt_pipeline_bytes(const sbwt_index *index, uint64_t *h2d, uint64_t *d2h);
+
 /* Membership only: as sbwt_search_reads_host, but the result is the bitmap
  * member_bits (host, ceil(n_kmers/32) u32 words; bit j%32 of word j/32 =
  * k-mer j is indexed) and no answer array crosses the bus (1 bit instead of

@@ -150,6 +150,13 @@ class Index:
         check(lib.sbwt_build_times(self._h, ms))
         return {"lines_ms": ms[0], "poppy_ms": ms[1], "presearch_ms": ms[2], "backward_ms": ms[3]}
 
+    def pipeline_bytes(self):
+        """Bytes the last host-buffer search (search_reads_host, member_reads_host) copied
+        host->device and device->host."""
+        h2d, d2h = ctypes.c_uint64(0), ctypes.c_uint64(0)
+        check(lib.sbwt_pipeline_bytes(self._h, ctypes.byref(h2d), ctypes.byref(d2h)))
+        return {"h2d": h2d.value, "d2h": d2h.value}
+
     def set_search_mode(self, mode):
         """SEARCH_EVERY_KMER, SEARCH_SKIP_ABSENT or SEARCH_STREAM (default) for searches of reads;
         the answers are the same in every mode."""

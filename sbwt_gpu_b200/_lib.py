@@ -116,6 +116,7 @@ SIGNATURES = {
     "sbwt_index_info": (c_int, [c_void_p, POINTER(c_uint64), POINTER(c_uint64), POINTER(c_uint32), POINTER(c_uint32)]),
     "sbwt_presearch": (c_int, [c_void_p, c_uint32]),
     "sbwt_build_times": (c_int, [c_void_p, POINTER(ctypes.c_float)]),
+    "sbwt_pipeline_bytes": (c_int, [c_void_p, POINTER(ctypes.c_uint64), POINTER(ctypes.c_uint64)]),
     "sbwt_presearch_export": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64]),
     "sbwt_rank_export": (c_int, [c_void_p, c_uint32, c_int32, c_int, c_void_p, c_uint64, c_void_p, c_uint64]),
     "sbwt_configure": (c_int, [c_void_p, c_int32, c_uint32, c_int32, c_int32, c_uint32, c_uint32, c_uint32]),

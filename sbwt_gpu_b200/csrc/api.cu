@@ -352,6 +352,14 @@ extern "C" int sbwt_build_times(const sbwt_index *ix, float ms[4]) {
     return 0;
 }
 
+extern "C" int sbwt_pipeline_bytes(const sbwt_index *ix, uint64_t *h2d, uint64_t *d2h) {
+    clear_error();
+    if (!ix || !h2d || !d2h) return set_error("NULL argument");
+    *h2d = ix->pipe_h2d;
+    *d2h = ix->pipe_d2h;
+    return 0;
+}
+
 extern "C" int sbwt_presearch_export(const sbwt_index *ix, uint64_t *lefts, uint64_t *rights, uint64_t count) {
     clear_error();
     if (!ix || !lefts || !rights) return set_error("NULL argument");

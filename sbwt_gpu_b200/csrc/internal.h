@@ -137,9 +137,11 @@ struct sbwt_index {
     size_t scan_cap = 0;
     // per-call work buffers: ws[0] serves the device-pointer entry points,
     // ws[0 .. kPipeSlots) the streams of the host pipeline
-    static constexpr int kPipeSlots = 3;
+    static constexpr int kPipeSlots = 4;
     sbwt::Workspace ws[kPipeSlots];
-    cudaStream_t pipe_stream[kPipeSlots] = {nullptr, nullptr, nullptr};
+    cudaStream_t pipe_stream[kPipeSlots] = {nullptr, nullptr, nullptr, nullptr};
+    // bytes the last host-pipeline call copied host->device and device->host
+    uint64_t pipe_h2d = 0, pipe_d2h = 0;
     // bumped whenever a device structure a search reads is rebuilt (graph keys)
     uint64_t gen = 1;
     bool use_graph = false;

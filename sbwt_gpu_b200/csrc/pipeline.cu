@@ -1,5 +1,5 @@
 // pipeline.cu -- sbwt_search_reads_host: a batch of reads in host memory is
-// streamed through the GPU in chunks of rows.  Three CUDA streams take
+// streamed through the GPU in chunks of rows.  Four CUDA streams take
 // turns; on each, a chunk's letters and row table go host->device, the chunk
 // is packed and searched, and its answers come back device->host, so the
 // copies of one chunk overlap the search of another while the host prepares
@@ -9,9 +9,11 @@
 // device->host copy the bound): while node ids fit in 32 bits and at least
 // six host threads can expand them, a chunk comes back as its membership
 // bitmap, per-group offsets and the found node ids, and the host threads
-// expand them into the caller's answers.  Per chunk b
-// the loop issues b, starts the node-id copy of b-1 (its count is known once
-// b-1's bitmap and offsets are in) and expands b-2.
+// expand them into the caller's answers.  Per chunk b the loop issues b,
+// starts the node-id copy of b-2 (its count is known once b-2's bitmap and
+// offsets are in) and expands b-3, so that two chunks keep the copy engines
+// and the GPU busy while the host threads expand.  Hybrid: every fourth
+// chunk's u64 answers go by DMA into the caller's pinned buffer instead.
 //
 // This replaces the strictly sequential host<->device chain of the reference
 // (KmerSearch::search, include/epicseq/kmer_search.hpp:97-160: one H2D of the
@@ -75,17 +77,27 @@ u64 chunk_letters() {
 // 0.125 + 4 x (found fraction) bytes per k-mer instead of 8.  The host
 // expands them into the u64 answers (~0 for an absent k-mer).
 constexpr u32 kGroupWords = 64;
-constexpr int kMinExpandThreads = 6;
-
-// The environment variable SBWT_PIPELINE_TRANSFER = "dense" or "sparse"
-// overrides the choice by thread count.
-bool sparse_transfer() {
-    const char *e = std::getenv("SBWT_PIPELINE_TRANSFER");
-    if (e && std::strcmp(e, "dense") == 0) return false;
-    if (e && std::strcmp(e, "sparse") == 0) return true;
-    return omp_get_max_threads() >= kMinExpandThreads;
-}
 constexpr u32 kGroupWarps = 4;  // groups (warps) per block of group_nodes_kernel
+
+// How a chunk's answers cross PCIe: u64 answers (dense), the sparse form, or
+// both (hybrid: every kHybridPeriod-th chunk dense, copied straight into the
+// caller's pinned buffer by the copy engines while the host threads expand
+// the sparse ones).  Sparse needs 32-bit node ids and enough host threads
+// to expand faster than PCIe brings u64 answers (about 11 GB/s of answers
+// per thread against 57 GB/s).  The environment variable
+// SBWT_PIPELINE_TRANSFER = dense | sparse | hybrid overrides the choice.
+enum Transfer { kDense, kSparse, kHybrid };
+constexpr int kMinExpandThreads = 6;
+constexpr u64 kHybridPeriod = 4;
+
+Transfer transfer_mode(const sbwt_index *ix) {
+    if (ix->n > 0xffffffffull) return kDense;
+    const char *e = std::getenv("SBWT_PIPELINE_TRANSFER");
+    if (e && std::strcmp(e, "dense") == 0) return kDense;
+    if (e && std::strcmp(e, "sparse") == 0) return kSparse;
+    if (e && std::strcmp(e, "hybrid") == 0) return kHybrid;
+    return omp_get_max_threads() >= kMinExpandThreads ? kSparse : kDense;
+}
 
 // gcnt[g] = found k-mers of group g; gcnt[ng] = 0 (the exclusive scan's total).
 __global__ void group_count_kernel(const uint32_t *__restrict__ member, u64 nw, u64 ng, u64 *__restrict__ gcnt) {
@@ -225,11 +237,14 @@ int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, con
     for (int i = 0; i < kSlots; i++)
         if (!ix->pipe_stream[i]) SBWT_CHECK_CUDA(cudaStreamCreateWithFlags(&ix->pipe_stream[i], cudaStreamNonBlocking));
     const bool pin_in = is_pinned(letters);
-    // answers leave the device in sparse form while node ids fit in 32 bits
-    // and enough host threads expand them faster than PCIe brings u64
-    // answers (about 11 GB/s of answers per thread against 57 GB/s)
-    const bool sparse = answers && ix->n <= 0xffffffffull && sparse_transfer();
-    const bool pin_out = answers && !sparse && (n_kmers == 0 || is_pinned(answers));
+    const Transfer xfer = answers ? transfer_mode(ix) : kDense;
+    const bool sparse = xfer != kDense;  // some chunks come back in sparse form
+    const bool pin_out = answers && (n_kmers == 0 || is_pinned(answers));
+    // dense chunks: all of them, or (hybrid, into a pinned buffer) every kHybridPeriod-th
+    auto dense_chunk = [&](size_t b) {
+        return xfer == kDense || (xfer == kHybrid && pin_out && b % kHybridPeriod == kHybridPeriod - 1);
+    };
+    ix->pipe_h2d = ix->pipe_d2h = 0;
     u64 max_letters = 0, max_rows = 0, max_k = 0;
     for (const Chunk &c : chunks) {
         max_letters = std::max(max_letters, c.l1 - c.l0);
@@ -287,6 +302,7 @@ int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, con
         if (found)
             SBWT_CHECK_CUDA(cudaMemcpyAsync(w.h_nodes, w.nodes, found * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                                             ix->pipe_stream[slot]));
+        ix->pipe_d2h += found * sizeof(uint32_t);
         return 0;
     };
     auto drain = [&](int slot) -> int {
@@ -332,6 +348,7 @@ int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, con
 #pragma omp parallel for schedule(static) if (nr > (1u << 16))
         for (int64_t r = 0; r <= (int64_t)nr; r++) hr[r] = row_starts[c.r0 + r] - c.l0;
         SBWT_CHECK_CUDA(cudaMemcpyAsync(w.rows, w.h_rows, (nr + 1) * sizeof(u64), cudaMemcpyHostToDevice, s));
+        ix->pipe_h2d += (nr + 1) * sizeof(u64) + nl;
         if (pin_in) {
             SBWT_CHECK_CUDA(cudaMemcpyAsync(w.letters, letters + c.l0, nl, cudaMemcpyHostToDevice, s));
         } else {
@@ -339,7 +356,7 @@ int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, con
             SBWT_CHECK_CUDA(cudaMemcpyAsync(w.letters, w.h_letters, nl, cudaMemcpyHostToDevice, s));
         }
         stage[slot] = 1;
-        if (sparse) {
+        if (answers && !dense_chunk(b)) {
             // answers and bitmap in one search, then the found node ids gathered per group
             SBWT_TRY(search_rows_device(ix, w, w.letters, nl, w.rows, nr, w.answers, w.member, c.nk, s));
             if (c.nk) {
@@ -357,14 +374,13 @@ int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, con
                 SBWT_CHECK_CUDA(cudaGetLastError());
                 SBWT_CHECK_CUDA(cudaMemcpyAsync(w.h_member, w.member, nw * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
                 SBWT_CHECK_CUDA(cudaMemcpyAsync(w.h_goff, goff, (ng + 1) * sizeof(u64), cudaMemcpyDeviceToHost, s));
+                ix->pipe_d2h += nw * sizeof(uint32_t) + (ng + 1) * sizeof(u64);
                 pending[slot] = (long)b;
             }
-            // the previous chunk's node ids start on their way; the one before is expanded
-            if (b >= 1) SBWT_TRY(fetch_nodes((int)((b - 1) % kSlots)));
-            if (b >= 2) SBWT_TRY(drain((int)((b - 2) % kSlots)));
         } else if (answers) {
             SBWT_TRY(search_rows_device(ix, w, w.letters, nl, w.rows, nr, w.answers, nullptr, c.nk, s));
             if (c.nk) {
+                ix->pipe_d2h += c.nk * sizeof(u64);
                 if (pin_out) {
                     SBWT_CHECK_CUDA(cudaMemcpyAsync(answers + c.k0, w.answers, c.nk * sizeof(u64),
                                                     cudaMemcpyDeviceToHost, s));
@@ -378,7 +394,14 @@ int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, con
             SBWT_TRY(search_rows_device(ix, w, w.letters, nl, w.rows, nr, nullptr, w.member, c.nk, s));
             SBWT_CHECK_CUDA(cudaMemcpyAsync(w.h_member, w.member, (c.nk + 31) / 32 * sizeof(uint32_t),
                                             cudaMemcpyDeviceToHost, s));
+            ix->pipe_d2h += (c.nk + 31) / 32 * sizeof(uint32_t);
             pending[slot] = (long)b;
+        }
+        if (sparse) {
+            // node ids of chunk b-2 start on their way (its bitmap and offsets have had a whole
+            // iteration to arrive); chunk b-3's are in, it is expanded while b-1 and b run
+            if (b >= 2) SBWT_TRY(fetch_nodes((int)((b - 2) % kSlots)));
+            if (b >= 3) SBWT_TRY(drain((int)((b - 3) % kSlots)));
         }
     }
     // the chunks still in flight, oldest first

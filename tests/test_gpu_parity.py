@@ -484,14 +484,15 @@ def test_host_pipelines_across_chunks(small, cuda):
     assert np.array_equal(mem, _bits_of(want))
 
 
-@pytest.mark.parametrize("transfer", ["sparse", "dense"])
+@pytest.mark.parametrize("transfer", ["sparse", "dense", "hybrid"])
 @pytest.mark.parametrize("chunk", [4096, 50_000])
 def test_host_answers_sparse_transfer_many_chunks(small, cuda, monkeypatch, chunk, transfer):
     """The host answers pipeline brings a chunk's answers back as its membership bitmap, group
     offsets and found node ids and expands them on the host (or, dense, as u64 answers).  Many
-    chunks (every stage of the three-slot rotation), chunks where every k-mer is found (genome
+    chunks (every stage of the four-slot rotation), chunks where every k-mer is found (genome
     reads only), reads without a found k-mer, ragged, empty and shorter-than-k rows, against the
     oracle."""
+    import torch
     b, k = small["built"], small["k"]
     rng = wl.rng_for(91)
     g = small["genome"]
@@ -517,8 +518,14 @@ def test_host_answers_sparse_transfer_many_chunks(small, cuda, monkeypatch, chun
     monkeypatch.setenv("SBWT_PIPELINE_TRANSFER", transfer)
     with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=10) as ix:
         host = ix.search_reads_host(letters, rows)
+        moved = ix.pipeline_bytes()
+        pa = torch.empty(want.size, dtype=torch.int64).pin_memory()  # hybrid copies into pinned buffers
+        ix.search_reads_host(letters, rows, pa)
         mem = ix.member_reads_host(letters, rows)
     assert letters.size > 2 * chunk
+    assert moved["h2d"] > letters.size and 0 < moved["d2h"]
+    assert (moved["d2h"] >= 8 * want.size) == (transfer == "dense")
+    assert np.array_equal(pa.numpy().view(np.uint64), want)
     assert (want != orc.NOT_FOUND).mean() > 0.3 and (want == orc.NOT_FOUND).any()
     assert np.array_equal(host, want)
     assert np.array_equal(mem, _bits_of(want))
