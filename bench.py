@@ -308,6 +308,18 @@ def kernel_traffic(kernel, workload, n_kmers):
     return None, None
 
 
+def host_threads_per_rank(world, impl):
+    """torchrun gives every rank OMP_NUM_THREADS=1 unless it is set; the host threads (answer
+    expansion, the CPU arms) get their share of the cores instead: all of them for the reference
+    arm (rank 0 alone runs), cores / ranks on this node for this project's arm.  Must run before
+    the first OpenMP runtime starts in this process."""
+    if world <= 1 or os.environ.get("OMP_NUM_THREADS", "") not in ("", "1"):
+        return
+    cores = len(os.sched_getaffinity(0))
+    local = int(os.environ.get("LOCAL_WORLD_SIZE", str(world)))
+    os.environ["OMP_NUM_THREADS"] = str(cores if impl == "reference" else max(1, cores // max(local, 1)))
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -315,6 +327,7 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     k = 31
     p = args.p
+    host_threads_per_rank(world, args.impl)
 
     if args.impl == "reference":
         if rank != 0:

@@ -77,3 +77,17 @@ def test_reference_arm_under_torchrun_prints_one_line():
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] > 0 and d["e2e"]["h2d_bytes_per_step"] == 0
+    # torchrun's OMP_NUM_THREADS=1 does not reach the reference arm: rank 0 runs on every core
+    assert d["cpu_baseline"]["cores"] == len(os.sched_getaffinity(0))
+
+
+def test_host_threads_per_rank(monkeypatch):
+    import bench as b
+    cores = len(os.sched_getaffinity(0))
+    for impl, world, local, env, want in [("ours", 1, 1, "", ""), ("ours", 2, 2, "1", str(max(1, cores // 2))),
+                                          ("reference", 2, 2, "1", str(cores)), ("ours", 2, 2, "3", "3"),
+                                          ("ours", 4, 2, "", str(max(1, cores // 2)))]:
+        monkeypatch.setenv("OMP_NUM_THREADS", env)
+        monkeypatch.setenv("LOCAL_WORLD_SIZE", str(local))
+        b.host_threads_per_rank(world, impl)
+        assert os.environ["OMP_NUM_THREADS"] == want, (impl, world, env)
