@@ -306,6 +306,7 @@ extern "C" void sbwt_index_free(sbwt_index *ix) {
     cudaFree(ix->d_L0);
     cudaFree(ix->d_L12);
     cudaFree(ix->d_pre);
+    cudaFree(ix->d_pre32);
     cudaFree(ix->d_scan);
     cudaFree(ix->d_node);
     cudaFree(ix->d_sel);
@@ -453,6 +454,7 @@ SearchArgs base_args(const sbwt_index *ix, bool rows) {
     a.chunk = search_chunk(ix, rows);
     a.runs = rows && runs_form(ix);
     a.stream = a.runs && stream_form(ix);
+    a.pre32 = a.runs ? ix->d_pre32 : nullptr;
     if (a.stream) a.sv = stream_view(ix);
     set_gather_policies(ix, a);
     return a;

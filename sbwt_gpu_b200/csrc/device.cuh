@@ -84,6 +84,20 @@ __device__ __forceinline__ u64 l2_evict_first_policy() {
     return p;
 }
 
+// Compact presearch entry (one u32): left end L in the low kPreLBits bits,
+// width w = R - L + 1 above it; w = 0 is an empty interval and w =
+// kPreEscape means the interval is too wide for the field (the 8-byte entry
+// holds it).  Halves the table, so that at p = 12 (64 MiB) it can stay in L2.
+constexpr u32 kPreLBits = 27;
+constexpr u32 kPreEscape = 31;
+constexpr u64 kPreMaxColumns = 1ull << kPreLBits;
+
+__host__ __device__ __forceinline__ u32 pre_compact(u32 l, u32 r) {
+    if (l > r) return 0u;
+    const u32 w = r - l + 1u;
+    return l | ((w < kPreEscape ? w : kPreEscape) << kPreLBits);
+}
+
 // A gather: with the evict-first policy pol when ef is set, plainly otherwise.
 __device__ __forceinline__ uint2 ld_gather_u32x2(const uint2 *p, bool ef, u64 pol) {
 #if SBWT_GATHER_EVICT_FIRST

@@ -26,6 +26,8 @@ struct SearchArgs {
     // common
     u64 C[5];
     const void *pre;  // presearch table: uint2 (n < 2^32) or ulonglong2 entries; NULL if p == 0
+    // with `runs`: the compact presearch table (one u32 an entry, below) or NULL
+    const uint32_t *pre32;
     u32 p;
     u32 k;
     const u64 *words;       // packed letters
@@ -121,6 +123,10 @@ struct sbwt_index {
     // presearch table
     uint32_t p = 0;
     void *d_pre = nullptr;
+    // compact presearch table for the run walk (indexes below 2^27 columns):
+    // entry = L | w << 27, w = R - L + 1 (0: empty interval, kPreEscape: look
+    // the entry up in d_pre, the interval is wider than the field holds)
+    uint32_t *d_pre32 = nullptr;
     bool pre64 = false;
     // backward-step structures (stream.cu): node nibbles, select samples, backward table
     uint8_t *d_node = nullptr;

@@ -487,9 +487,20 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
                 const u32 sh = (u32)(b & 63u);
                 kmer = (w0 << sh) | (shr_clamp(w1, 63u - sh) >> 1);
                 if (p) {
-                    const PT e = ld_gather_u32x2(pre + (kmer >> (64u - 2u * p)), a.ef_pre, gpol);
-                    L = e.x;
-                    Rr = e.y;
+                    const u64 idx = kmer >> (64u - 2u * p);
+                    u32 w = kPreEscape;
+                    if (a.pre32) {  // compact entry; the 8-byte one only for intervals too wide for it
+                        const u32 c = __ldg(a.pre32 + idx);
+                        w = c >> kPreLBits;
+                        L = c & ((1u << kPreLBits) - 1u);
+                        Rr = L + w - 1u;
+                        if (w == 0) L = 1u, Rr = 0u;
+                    }
+                    if (w == kPreEscape) {
+                        const PT e = ld_gather_u32x2(pre + idx, a.ef_pre, gpol);
+                        L = e.x;
+                        Rr = e.y;
+                    }
                 } else {
                     L = 0;
                     Rr = rootR;

@@ -531,6 +531,27 @@ def test_host_answers_sparse_transfer_many_chunks(small, cuda, monkeypatch, chun
     assert np.array_equal(mem, _bits_of(want))
 
 
+@pytest.mark.parametrize("compact", ["1", "0"])
+@pytest.mark.parametrize("p", [2, 6, 10, 13])
+def test_run_walk_compact_presearch_entries(small, cuda, monkeypatch, p, compact):
+    """The run walk reads 4-byte presearch entries (left end + width) and the 8-byte entry only
+    for intervals too wide for the width field: p = 2 (every interval wide), 6 (both kinds),
+    10 and 13 (narrow and empty ones), with and without the compact table."""
+    monkeypatch.setenv("SBWT_PRESEARCH_COMPACT", compact)
+    b, k = small["built"], small["k"]
+    want = orc.OracleIndex(b.bits, b.n_bits).search_reads(small["letters"], small["rows"], k, p)
+    with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=p) as ix:
+        for mode in (sg.SEARCH_SKIP_ABSENT, sg.SEARCH_STREAM):
+            ix.set_search_mode(mode)
+            assert np.array_equal(run_reads(ix, small["letters"], small["rows"], cuda), want), mode
+    lefts, rights = orc.OracleIndex(b.bits, b.n_bits).presearch(p)
+    width = np.where(lefts <= rights, rights.astype(np.int64) - lefts.astype(np.int64) + 1, 0)
+    if p == 2:
+        assert (width >= 31).all()
+    if p == 6:
+        assert (width >= 31).any() and ((width > 0) & (width < 31)).any()
+
+
 def test_build_times_reported(small, cuda):
     b = small["built"]
     with sg.Index.from_bits(b.bits, b.n_bits, k=31, k_presearch=10) as ix:
