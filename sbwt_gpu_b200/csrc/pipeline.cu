@@ -190,8 +190,8 @@ namespace {
 
 // The pipeline behind both host entry points: exactly one of `answers`
 // (u64 per k-mer) and `member` (bit j%32 of word j/32) is non-NULL.
-int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, const uint64_t *row_starts,
-                 uint64_t n_rows, uint64_t *answers, uint32_t *member, uint64_t n_kmers) {
+int pipeline_chunks(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, const uint64_t *row_starts,
+                    uint64_t n_rows, uint64_t *answers, uint32_t *member, uint64_t n_kmers) {
     if (!ix) return set_error("index is NULL");
     if (n_rows == 0) return 0;
     if (!letters || !row_starts || (n_kmers && !answers && !member)) return set_error("NULL host pointer");
@@ -407,6 +407,17 @@ int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, con
     // the chunks still in flight, oldest first
     for (size_t i = 0; i < (size_t)kSlots; i++) SBWT_TRY(drain((int)((chunks.size() + i) % kSlots)));
     return 0;
+}
+
+// An error leaves no copy or kernel of the call in flight: the next call
+// reuses the buffers they would write.
+int run_pipeline(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, const uint64_t *row_starts,
+                 uint64_t n_rows, uint64_t *answers, uint32_t *member, uint64_t n_kmers) {
+    const int rc = pipeline_chunks(ix, letters, n_letters, row_starts, n_rows, answers, member, n_kmers);
+    if (rc && ix)
+        for (cudaStream_t st : ix->pipe_stream)
+            if (st) cudaStreamSynchronize(st);
+    return rc;
 }
 
 }  // namespace
