@@ -149,7 +149,9 @@ __global__ void __launch_bounds__(32 * kGroupWarps) group_nodes_kernel(const uin
 }
 
 // answers[j] for the nk k-mers of one chunk from its sparse form (streaming
-// stores: the answers are not read back by this thread).
+// stores: the answers are not read back by this thread).  nodes may be read
+// one element past the chunk's found ids (a select instead of a branch), so
+// its buffer has slack.
 void expand_answers(u64 *answers, u64 nk, const uint32_t *member, const u64 *goff, const uint32_t *nodes) {
     const u64 nw = (nk + 31) / 32, ng = (nw + kGroupWords - 1) / kGroupWords;
 #pragma omp parallel if (nk > (1u << 16))
@@ -275,7 +277,7 @@ int pipeline_chunks(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, 
             SBWT_TRY(grow(w.goff, w.goff_cap, max_groups + 1 + scan_words));
             SBWT_TRY(grow(w.nodes, w.nodes_cap, max_k));
             SBWT_TRY(grow_host(w.h_goff, w.h_goff_cap, max_groups + 1));
-            SBWT_TRY(grow_host(w.h_nodes, w.h_nodes_cap, max_k));
+            SBWT_TRY(grow_host(w.h_nodes, w.h_nodes_cap, max_k + 32));  // slack: expand_answers may read one past
         }
     }
     if (member) std::memset(member, 0, (n_kmers + 31) / 32 * sizeof(uint32_t));
