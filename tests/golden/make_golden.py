@@ -5,7 +5,7 @@ its own program (oracle/_ref/search: src/search.cpp built for sm_100a by
 oracle/Makefile) on seeded inputs and recording its stdout.
 
     python tests/golden/make_golden.py prepare   # CPU: write the inputs under tests/golden/cases/
-    python tests/golden/make_golden.py run OUT   # GPU box: run the reference on every case into OUT/
+    python tests/golden/make_golden.py run OUT   # on a B200: run the reference on every case into OUT/
     python tests/golden/make_golden.py collect OUT  # CPU: store OUT/<case>.out as fixtures
 
 Every case keeps the reference's in-bounds conditions (checked by
