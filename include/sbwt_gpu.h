@@ -39,6 +39,14 @@ extern "C" {
 /* Search layouts of this engine. */
 #define SBWT_LAYOUT_LINES 0 /* 32-byte lines: 32-bit rank word + 224 bits (default) */
 #define SBWT_LAYOUT_POPPY 1 /* the reference's L0/L12 poppy layout (bits_in_superblock, rank_structure) */
+/* Wider interleave blocks: 512-bit (64-byte) and 2048-bit (256-byte) lines, each a
+ * 32-bit rank word plus 16-bit counts per 32-byte sector and the block's bits, so a
+ * rank reads the line's first sector and the one holding its bit (batches of reads
+ * with the queue-fed kernels: kmers_per_thread 0, threads_per_kmer 1).  The
+ * reference's block-size axis is its superblock size (include/parameters.hpp:13-37,
+ * include/epicseq/search_caller.hpp:81-209). */
+#define SBWT_LAYOUT_LINES512 2
+#define SBWT_LAYOUT_LINES2048 3
 
 typedef struct sbwt_index sbwt_index;
 
@@ -52,7 +60,7 @@ typedef struct {
     int32_t with_shuffles;       /* cooperative rank for the poppy layout (parameters.hpp:45) */
     uint32_t threads_per_block;  /* 0 = engine default (parameters.hpp:51) */
     int32_t device;              /* CUDA device ordinal (the reference uses 0, parameters.hpp:81) */
-    int32_t layout;              /* SBWT_LAYOUT_LINES | SBWT_LAYOUT_POPPY */
+    int32_t layout;              /* SBWT_LAYOUT_LINES | _POPPY | _LINES512 | _LINES2048 */
     uint32_t kmers_per_thread;   /* search kernel: 0 = one k-mer per lane fed from a per-warp queue
                                     (default); 1,2,3,4,6,8 = k-mer slots held in registers */
     uint32_t threads_per_kmer;   /* search kernel: lanes sharing one k-mer, 1|2|4 (0 = default) */
@@ -211,17 +219,20 @@ int sbwt_pack(const uint8_t *d_letters, uint64_t n_letters, uint64_t *d_words, v
 int sbwt_search_reads(sbwt_index *index, const uint8_t *d_letters, uint64_t n_letters, const uint64_t *d_row_starts,
                       uint64_t n_rows, uint64_t *d_answers, uint32_t *d_member_bits, uint64_t n_kmers, void *stream);
 
-/* sbwt_search_reads for callers that cannot allocate device memory at search
- * time: one capturing the search into its own CUDA graph (cudaMalloc cannot be
- * captured), or one whose device memory another allocator already holds.  No
- * counterpart in the reference.  Same arguments and answers as
- * sbwt_search_reads, but all scratch (packed letters, per-row k-mer table,
- * chunk table, scan sums, work counter) lives in one fixed 32 MiB device array
- * of the library (held by every GPU that loads it until exit), so no
- * cudaMalloc/cudaFree is made; a batch needing more (roughly more than 64M
- * letters) is rejected with an error.  The first call on a device looks the
- * array up (cudaGetSymbolAddress): make it before any stream capture.  Calls
- * share the array: calls that overlap on the GPU race. */
+/* sbwt_search_reads for callers that cannot call cudaMalloc while they
+ * search: a process whose device memory another allocator already holds (a
+ * framework's caching allocator that reserved the GPU), or an application
+ * that accounts for every device allocation itself.  No counterpart in the
+ * reference.  Same arguments and answers as sbwt_search_reads (d_answers may
+ * be NULL when d_member_bits is given), but all scratch (packed letters,
+ * per-row k-mer table, chunk table, scan sums, work counter, and the answers
+ * of a membership-only search with the per-k-mer kernels) lives in one fixed
+ * 32 MiB device array of the library (held by every GPU that loads it until
+ * exit), so no cudaMalloc/cudaFree is made.  A batch needing more is rejected
+ * with an error giving the bytes it needs: about 100M letters of 150-letter
+ * reads fit, fewer when the rows are shorter.  The first call on a device looks
+ * the array up (cudaGetSymbolAddress): make it before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race. */
 int sbwt_search_reads_noalloc(sbwt_index *index, const uint8_t *d_letters, uint64_t n_letters,
                               const uint64_t *d_row_starts, uint64_t n_rows, uint64_t *d_answers,
                               uint32_t *d_member_bits, uint64_t n_kmers, void *stream);
@@ -344,6 +355,24 @@ int sbwt_search_kmers(sbwt_index *index, const uint64_t *d_kmers, uint64_t n, ui
  * answered without a search. */
 int sbwt_search_kmers_filtered(sbwt_index *index, sbwt_prefilter *pf, const uint64_t *d_kmers, uint64_t n,
                                uint64_t *d_answers, uint64_t *n_skipped, void *stream);
+
+/* sbwt_search_reads behind the learned prefilter (the learned-Bloom
+ * sandwich): the model classifies every k-mer of the batch (its logit
+ * against tau) and the backup Bloom filter, built over every indexed k-mer
+ * the model rejects, is probed for the rejected ones; a k-mer rejected by
+ * both is answered absent (~0) without a search, every other k-mer is
+ * searched exactly, so no indexed k-mer is ever reported absent and the
+ * answers equal sbwt_search_reads'.  Same arguments as sbwt_search_reads
+ * plus the prefilter (trained on this index, same k); *n_skipped (optional,
+ * synchronizes) = k-mers answered from the prefilter alone.  Needs the run
+ * walk on the line layout (search mode stream or skip).  Scratch: 8 bytes per
+ * k-mer of a 64M-k-mer inference chunk and one bit per k-mer, grown on the
+ * prefilter handle.  In front of the reference's search kernel
+ * (include/gpu/search_kernel.hpp:61-104, fed by include/epicseq/
+ * kmer_search.hpp:97-153), which has no prefilter. */
+int sbwt_search_reads_filtered(sbwt_index *index, sbwt_prefilter *pf, const uint8_t *d_letters, uint64_t n_letters,
+                               const uint64_t *d_row_starts, uint64_t n_rows, uint64_t *d_answers,
+                               uint32_t *d_member_bits, uint64_t n_kmers, uint64_t *n_skipped, void *stream);
 
 /* Test hooks of the training kernels: loss and gradient of one BCE step for
  * the given parameters and batch (n a multiple of 256), and the logits of

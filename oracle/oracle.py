@@ -50,6 +50,7 @@ def _load():
         "orc_rank": (c_uint64, [P, P, P, c_uint32, c_int, c_uint64]),
         "orc_c_array": (None, [P, P]),
         "orc_presearch": (None, [P, P, P, P, c_uint32, c_int, c_uint32, P, P]),
+        "orc_presearch_at": (None, [P, P, P, P, c_uint32, c_int, c_uint32, P, c_uint64, P, P]),
         "orc_read_queries": (c_int64, [P, c_uint64, c_uint32, P, P, P, P]),
         "orc_pack": (None, [P, c_uint64, P]),
         "orc_positions": (c_uint64, [P, c_uint64, c_uint32, P]),
@@ -152,6 +153,15 @@ class OracleIndex:
         lib.orc_presearch(_ptrs(self.words), _ptrs(self.L0), _ptrs(self.L12), _p(self.C), self.sb, self.kind, p,
                           _p(lefts), _p(rights))
         return lefts, rights
+
+    def presearch_at(self, p, idx):
+        """Entries of the p-mers idx (uint64 array) of the presearch table."""
+        idx = np.ascontiguousarray(idx, dtype=np.uint64)
+        lefts = np.zeros(max(idx.size, 1), dtype=np.uint64)
+        rights = np.zeros(max(idx.size, 1), dtype=np.uint64)
+        lib.orc_presearch_at(_ptrs(self.words), _ptrs(self.L0), _ptrs(self.L12), _p(self.C), self.sb, self.kind, p,
+                             _p(idx), idx.size, _p(lefts), _p(rights))
+        return lefts[: idx.size], rights[: idx.size]
 
     def search_positions(self, words, positions, k, p, table=None, want_steps=False):
         """search_kernel.hpp:61-104 over packed words + positions."""

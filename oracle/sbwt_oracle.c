@@ -235,27 +235,49 @@ static inline u64 rank_c(const orc_index *ix, u32 c, u64 i)
 }
 
 /* a6: presearch kernel, presearch_kernel.hpp:19-37 (no early exit; an empty
- * interval stays empty).  Writes 4^p entries. */
+ * interval stays empty): the entry of p-mer idx (first letter in its top two
+ * bits). */
+static void presearch_entry(const orc_index *ix, u32 p, u64 idx, u64 *left, u64 *right)
+{
+    u32 c = (u32)((idx >> ((p - 1u) * 2u)) & 3u);
+    u64 l = ix->C[c], r = ix->C[c + 1] - 1ull;
+    for (int s = (int)((p - 2u) * 2u); s >= 0; s -= 2) {
+        c = (u32)((idx >> s) & 3u);
+        l = ix->C[c] + rank_c(ix, c, l);
+        r = ix->C[c] + rank_c(ix, c, r + 1ull) - 1ull;
+    }
+    *left = l;
+    *right = r;
+}
+
+static void presearch_index(orc_index *ix, const u64 *const data[4], const u64 *const L0[4],
+                            const u64 *const L12[4], const u64 C[5], u32 sb, int kind)
+{
+    for (int c = 0; c < 4; c++) { ix->data[c] = data[c]; ix->L0[c] = L0[c]; ix->L12[c] = L12[c]; }
+    memcpy(ix->C, C, sizeof(ix->C));
+    ix->sb = sb; ix->kind = kind;
+}
+
+/* Writes all 4^p entries. */
 void orc_presearch(const u64 *const data[4], const u64 *const L0[4], const u64 *const L12[4], const u64 C[5],
                    u32 sb, int kind, u32 p, u64 *lefts, u64 *rights)
 {
     orc_index ix;
-    for (int c = 0; c < 4; c++) { ix.data[c] = data[c]; ix.L0[c] = L0[c]; ix.L12[c] = L12[c]; }
-    memcpy(ix.C, C, sizeof(ix.C));
-    ix.sb = sb; ix.kind = kind;
+    presearch_index(&ix, data, L0, L12, C, sb, kind);
     const u64 count = 1ull << (2 * p);
 #pragma omp parallel for schedule(static)
-    for (u64 idx = 0; idx < count; idx++) {
-        u32 c = (u32)((idx >> ((p - 1u) * 2u)) & 3u);
-        u64 l = C[c], r = C[c + 1] - 1ull;
-        for (int s = (int)((p - 2u) * 2u); s >= 0; s -= 2) {
-            c = (u32)((idx >> s) & 3u);
-            l = C[c] + rank_c(&ix, c, l);
-            r = C[c] + rank_c(&ix, c, r + 1ull) - 1ull;
-        }
-        lefts[idx] = l;
-        rights[idx] = r;
-    }
+    for (u64 idx = 0; idx < count; idx++) presearch_entry(&ix, p, idx, lefts + idx, rights + idx);
+}
+
+/* The entries of the p-mers idx[0 .. count) only (tables too large to
+ * restate whole in a test). */
+void orc_presearch_at(const u64 *const data[4], const u64 *const L0[4], const u64 *const L12[4], const u64 C[5],
+                      u32 sb, int kind, u32 p, const u64 *idx, u64 count, u64 *lefts, u64 *rights)
+{
+    orc_index ix;
+    presearch_index(&ix, data, L0, L12, C, sb, kind);
+#pragma omp parallel for schedule(static)
+    for (u64 t = 0; t < count; t++) presearch_entry(&ix, p, idx[t], lefts + t, rights + t);
 }
 
 /* ------------------------------------------------------------------------ */

@@ -18,12 +18,13 @@ from ctypes import POINTER, byref, c_uint32, c_uint64, c_void_p
 
 import numpy as np
 
-from ._lib import (CLI_PATH, LIB_PATH, SBWT_CUM_POPPY, SBWT_LAYOUT_LINES, SBWT_LAYOUT_POPPY, SBWT_POPPY, Built,
+from ._lib import (CLI_PATH, LIB_PATH, SBWT_CUM_POPPY, SBWT_LAYOUT_LINES, SBWT_LAYOUT_LINES512, SBWT_LAYOUT_LINES2048,
+                   SBWT_LAYOUT_POPPY, SBWT_POPPY, Built,
                    MlpParams, Params, PrefilterStats, Profile, Queries, SbwtError, check, lib)
 
 __all__ = [
     "Index", "Params", "SbwtError", "build_sbwt", "write_index_files", "read_queries", "format_answers",
-    "count_kmers", "read_queries_many", "format_answers_device", "default_params", "SBWT_POPPY", "SBWT_CUM_POPPY", "SBWT_LAYOUT_LINES", "SBWT_LAYOUT_POPPY",
+    "count_kmers", "read_queries_many", "format_answers_device", "default_params", "SBWT_POPPY", "SBWT_CUM_POPPY", "SBWT_LAYOUT_LINES", "SBWT_LAYOUT_POPPY", "SBWT_LAYOUT_LINES512", "SBWT_LAYOUT_LINES2048",
     "LIB_PATH", "CLI_PATH", "NOT_FOUND", "SEARCH_EVERY_KMER", "SEARCH_SKIP_ABSENT", "SEARCH_STREAM", "Prefilter", "mlp_params", "mlp_gradients", "mlp_logits", "MLP_PARAMS",
 ]
 
@@ -222,6 +223,17 @@ class Index:
         check(lib.sbwt_search_kmers_filtered(self._h, prefilter._h, _ptr(d_kmers), n, _ptr(d_answers), byref(sk),
                                              _stream_ptr(stream)))
         return sk.value
+
+    def search_reads_filtered(self, prefilter, d_letters, d_row_starts, d_answers, n_kmers, d_member_bits=None,
+                              stream=None, count_skipped=True):
+        """search_reads behind the learned prefilter; returns the number of k-mers answered without a search
+        (None with count_skipped=False, which keeps the call asynchronous)."""
+        n_rows = int(d_row_starts.numel()) - 1
+        sk = c_uint64()
+        check(lib.sbwt_search_reads_filtered(self._h, prefilter._h, _ptr(d_letters), int(d_letters.numel()),
+                                             _ptr(d_row_starts), n_rows, _ptr(d_answers), _ptr(d_member_bits),
+                                             int(n_kmers), byref(sk) if count_skipped else None, _stream_ptr(stream)))
+        return sk.value if count_skipped else None
 
     def search_reads_host(self, letters, row_starts, answers=None):
         """Host reads -> host answers (numpy), streamed through the GPU."""

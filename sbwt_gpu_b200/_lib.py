@@ -9,13 +9,17 @@ import os
 from ctypes import POINTER, c_char_p, c_int, c_int32, c_int64, c_uint32, c_uint64, c_void_p
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libsbwt_gpu.so")
+# SBWT_GPU_LIBRARY names another build of the same library (for example one
+# compiled with different build options); the in-tree build otherwise.
+LIB_PATH = os.environ.get("SBWT_GPU_LIBRARY") or os.path.join(HERE, "libsbwt_gpu.so")
 CLI_PATH = os.path.join(HERE, "sbwt_search")
 
 SBWT_POPPY = 1
 SBWT_CUM_POPPY = 2
 SBWT_LAYOUT_LINES = 0
 SBWT_LAYOUT_POPPY = 1
+SBWT_LAYOUT_LINES512 = 2
+SBWT_LAYOUT_LINES2048 = 3
 
 
 class Params(ctypes.Structure):
@@ -144,6 +148,8 @@ SIGNATURES = {
     "sbwt_search_kmers": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_void_p]),
     "sbwt_search_kmers_filtered": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_void_p, POINTER(c_uint64),
                                            c_void_p]),
+    "sbwt_search_reads_filtered": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_void_p,
+                                           c_void_p, c_uint64, POINTER(c_uint64), c_void_p]),
     "sbwt_mlp_gradients": (c_int, [c_uint32, c_void_p, c_void_p, c_void_p, c_uint32, POINTER(ctypes.c_float),
                                    c_void_p]),
     "sbwt_mlp_logits": (c_int, [c_uint32, c_void_p, c_void_p, c_uint64, c_void_p]),

@@ -78,6 +78,7 @@ int use_device(int device) {
 int validate_params(const sbwt_params *p) {
     if (p->k < 3 || p->k > 32) return set_error("The value of k must be at least 3 and at most 32.");
     if (p->k_presearch > p->k) return set_error("presearch depth %u exceeds k = %u", p->k_presearch, p->k);
+    if (p->layout < SBWT_LAYOUT_LINES || p->layout > SBWT_LAYOUT_LINES2048) return set_error("unknown layout %d", p->layout);
     if (p->search_mode != SBWT_SEARCH_EVERY_KMER && p->search_mode != SBWT_SEARCH_SKIP_ABSENT &&
         p->search_mode != SBWT_SEARCH_STREAM)
         return set_error("unknown search mode %d", p->search_mode);
@@ -86,7 +87,7 @@ int validate_params(const sbwt_params *p) {
 
 void apply_shape(sbwt_index *ix, const sbwt_params *p) {
     sbwt::KernelShape &sh = ix->shape;
-    sh.layout = p->layout == SBWT_LAYOUT_POPPY ? SBWT_LAYOUT_POPPY : SBWT_LAYOUT_LINES;
+    sh.layout = (p->layout >= SBWT_LAYOUT_LINES && p->layout <= SBWT_LAYOUT_LINES2048) ? p->layout : SBWT_LAYOUT_LINES;
     // defaults from the autotuner on the large workload (1 k-mer per thread,
     // 128-thread blocks: occupancy beats register-resident k-mer slots)
     sh.kpt = p->kmers_per_thread;  // 0: the queue-fed single-slot kernel
@@ -158,7 +159,8 @@ int finish_index(sbwt_index *ix, const u64 *const words[4], const sbwt_params *p
         return set_error("the bit vectors are not an SBWT: 1 + total ones = %llu but n = %llu",
                          (unsigned long long)ix->C[4], (unsigned long long)n);
     apply_shape(ix, prm);
-    if (ix->shape.layout == SBWT_LAYOUT_LINES && !ix->lines_ok) ix->shape.layout = SBWT_LAYOUT_POPPY;
+    if (ix->shape.layout != SBWT_LAYOUT_POPPY && !ix->lines_ok) ix->shape.layout = SBWT_LAYOUT_POPPY;
+    if (sbwt::wide_sectors(ix->shape.layout)) SBWT_TRY(sbwt::build_wide(ix, sbwt::wide_sectors(ix->shape.layout), s));
     SBWT_CHECK_CUDA(cudaEventRecord(ev[2], s));
     SBWT_TRY(sbwt::run_presearch(ix, prm->k_presearch, s));
     SBWT_CHECK_CUDA(cudaEventRecord(ev[3], s));
@@ -303,6 +305,7 @@ extern "C" void sbwt_index_free(sbwt_index *ix) {
     cudaSetDevice(ix->device);
     cudaFree(ix->d_bits);
     cudaFree(ix->d_lines);
+    cudaFree(ix->d_wide);
     cudaFree(ix->d_L0);
     cudaFree(ix->d_L12);
     cudaFree(ix->d_pre);
@@ -390,9 +393,10 @@ extern "C" int sbwt_configure(sbwt_index *ix, int32_t layout, uint32_t sb, int32
     SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
     if (layout == SBWT_LAYOUT_POPPY) {
         if (!ix->poppy_ok || ix->sb != sb || ix->kind != kind) SBWT_TRY(build_poppy(ix, sb, kind, 0));
-    } else if (layout == SBWT_LAYOUT_LINES) {
+    } else if (layout == SBWT_LAYOUT_LINES || wide_sectors(layout)) {
         if (!ix->lines_ok) return set_error("the line layout is not available for an index of %llu columns",
                                             (unsigned long long)ix->n);
+        if (wide_sectors(layout) && ix->wide_s != wide_sectors(layout)) SBWT_TRY(build_wide(ix, wide_sectors(layout), 0));
     } else {
         return set_error("unknown layout %d", layout);
     }
@@ -430,11 +434,10 @@ void set_gather_policies(const sbwt_index *ix, SearchArgs &a) {
     const u64 half = ix->l2_bytes / 2;
     const u64 pre_bytes = ix->p ? (1ull << (2 * ix->p)) * (ix->pre64 ? 16ull : 8ull) : 0;
     const u64 back_bytes = ix->d_back ? ix->n * 8ull : 0;
-    a.ef_pre = a.runs && pre_bytes > half;
-    a.ef_back = a.runs && back_bytes > half;
+    const int ev = ix->shape.evict;
+    a.ef_pre = a.runs && ev != 1 && (ev == 2 || pre_bytes > half);
+    a.ef_back = a.runs && ev != 1 && (ev == 2 || back_bytes > half);
 }
-
-namespace {
 
 SearchArgs base_args(const sbwt_index *ix, bool rows) {
     SearchArgs a;
@@ -459,8 +462,6 @@ SearchArgs base_args(const sbwt_index *ix, bool rows) {
     set_gather_policies(ix, a);
     return a;
 }
-
-}  // namespace
 
 // Device-resident batch of rows on stream s using workspace w.
 int enqueue_rows(sbwt_index *ix, Workspace &w, SearchArgs &a, const uint8_t *d_letters, u64 n_letters, const u64 *d_rows,
@@ -520,6 +521,30 @@ int search_rows_device(sbwt_index *ix, Workspace &w, const uint8_t *d_letters, u
         SBWT_CHECK_CUDA(cudaGraphLaunch(w.graph, s));
     }
     return rc;
+}
+
+int prepare_rows(sbwt_index *ix, Workspace &w, SearchArgs &a, const uint8_t *d_letters, u64 n_letters,
+                 const u64 *d_rows, u64 n_rows, u64 n_kmers, cudaStream_t s) {
+    (void)ix;
+    const u64 n_words = (n_letters + 32 + 31) / 32;
+    SBWT_TRY(grow(w.words, w.words_cap, n_words));
+    SBWT_TRY(grow(w.kstart, w.kstart_cap, n_rows + 1));
+    SBWT_TRY(grow(w.scan, w.scan_cap, scan_scratch_words(n_rows)));
+    SBWT_TRY(grow(w.chunk_row, w.chunk_cap, (n_kmers + a.chunk - 1) / a.chunk));
+    SBWT_TRY(grow(w.counter, w.counter_cap, 1));
+    SBWT_TRY(launch_pack(d_letters, n_letters, w.words, s));
+    SBWT_TRY(launch_kstart(d_rows, n_rows, ix->k, w.kstart, w.scan, s));
+    SBWT_TRY(launch_chunk_rows(w.kstart, n_rows, n_kmers, a.chunk, w.chunk_row, s));
+    a.words = w.words;
+    a.positions = nullptr;
+    a.row_starts = d_rows;
+    a.kstart = w.kstart;
+    a.chunk_row = w.chunk_row;
+    a.n_rows = n_rows;
+    a.max_pos = (n_words - 1) * 32 - 1;
+    a.n_kmers = n_kmers;
+    a.counter = w.counter;
+    return 0;
 }
 
 // The kernels of one batch, in stream order.

@@ -202,6 +202,53 @@ __device__ __forceinline__ void line_split(u32 x, u32 &line, u32 &q) {
     q = x - line * kLineBits;
 }
 
+// ------------------------------------------------------------- wide lines
+//
+// WIDE lines: the interleave block widened to S sectors (S = 2: 512-bit
+// lines, S = 8: 2048-bit lines), with a two-level count so that a rank still
+// reads at most two sectors of its line.  Line bits (MSB-first across the
+// line's u64 words, as in LINES): [0, 32) the ones before the line (32-bit),
+// then S-1 16-bit fields sub[1..S-1] (sub[s] = ones of the line's data bits
+// that lie in sectors 0..s-1), then the data bits: data bit q at line bit
+// H + q, H = 32 + 16 (S-1).  rank_c(i) = count + sub[s] + the ones of sector
+// s before i's bit, s = the sector holding i's bit; the header sector and
+// that sector are independent loads.  Fewer count bits per data bit than
+// LINES (1.6 % at S = 8 against 14 %), one more sector per rank where the
+// bit lies past the first sector.
+template <int S> struct WideShape {
+    static constexpr u32 kSectors = S;
+    static constexpr u32 kHeaderBits = 32u + 16u * (S - 1);
+    static constexpr u32 kDataBits = 256u * S - kHeaderBits;
+};
+
+// Ones among the first b bits (MSB-first, b in [0, 256]) of a 256-bit sector.
+__device__ __forceinline__ u32 sector_prefix(const ulonglong4 &x, u32 b) {
+    const int t = (int)b;
+    return popc_top(x.x, clamp64(t)) + popc_top(x.y, clamp64(t - 64)) + popc_top(x.z, clamp64(t - 128)) +
+           popc_top(x.w, clamp64(t - 192));
+}
+
+__device__ __forceinline__ u64 sector_word(const ulonglong4 &x, u32 i) {
+    return i == 0 ? x.x : i == 1 ? x.y : i == 2 ? x.z : x.w;
+}
+
+// sub[s] of the header sector h (1 <= s < S).
+template <int S> __device__ __forceinline__ u32 wide_sub(const ulonglong4 &h, u32 s) {
+    const u32 b0 = 32u + 16u * (s - 1u);  // line bit of the field
+    return (u32)(sector_word(h, b0 >> 6) >> (48u - (b0 & 63u))) & 0xffffu;
+}
+
+// rank at data position q of a line (header sector h, x = the sector holding
+// q's bit, x = h when that is sector 0); *bit = the bit at q.
+template <int S> __device__ __forceinline__ u32 wide_rank(const ulonglong4 &h, const ulonglong4 &x, u32 q, u32 &bit) {
+    constexpr u32 H = WideShape<S>::kHeaderBits;
+    const u32 t = H + q, s = t >> 8, tb = t & 255u;
+    bit = (u32)(sector_word(x, tb >> 6) >> (63u - (tb & 63u))) & 1u;
+    const u32 before = s ? wide_sub<S>(h, s) : 0u;
+    const u32 in_sector = sector_prefix(x, tb) - (s ? 0u : sector_prefix(h, H));
+    return (u32)(h.x >> 32) + before + in_sector;
+}
+
 // ------------------------------------------------------------------ poppy
 
 template <int SB> struct PoppyShape {

@@ -84,6 +84,22 @@ __global__ void chunk_rows_kernel(const u64 *kstart, u64 n_rows, u64 n_chunks, u
     chunk_row[c] = (u32)lo;
 }
 
+// out[t] = the MSB-first 64-bit window of k-mer j0 + t of a batch of reads
+// (search_kernel.hpp:66-68 on the per-row k-mer table), t < count.
+__global__ void kmer_list_kernel(const u64 *__restrict__ words, const u64 *__restrict__ row_starts,
+                                 const u64 *__restrict__ kstart, const u32 *__restrict__ chunk_row, u32 chunk,
+                                 u64 max_pos, u64 j0, u64 count, u64 *__restrict__ out) {
+    const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const u64 j = j0 + t;
+    u64 r = chunk_row[j / chunk];
+    while (kstart[r + 1] <= j) r++;  // rows shorter than k hold no k-mers
+    const u64 b = min(row_starts[r] + (j - kstart[r]), max_pos) << 1;
+    const u64 w0 = words[b >> 6], w1 = words[(b >> 6) + 1];
+    const u32 sh = (u32)(b & 63u);
+    out[t] = (w0 << sh) | (dev::shr_clamp(w1, 63u - sh) >> 1);
+}
+
 __global__ void member_bits_kernel(const u64 *__restrict__ answers, u64 n, uint32_t *__restrict__ bits) {
     const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     const bool hit = i < n && answers[i] != ~0ull;
@@ -118,6 +134,14 @@ int launch_chunk_rows(const uint64_t *d_kstart, uint64_t n_rows, uint64_t n_kmer
     if (n_chunks == 0) return 0;
     chunk_rows_kernel<<<(unsigned)((n_chunks + 255) / 256), 256, 0, s>>>(d_kstart, n_rows, n_chunks, chunk,
                                                                          d_chunk_row);
+    SBWT_CHECK_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int launch_kmer_list(const SearchArgs &a, uint64_t j0, uint64_t count, uint64_t *d_out, cudaStream_t s) {
+    if (count == 0) return 0;
+    kmer_list_kernel<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(a.words, a.row_starts, a.kstart, a.chunk_row,
+                                                                     a.chunk, a.max_pos, j0, count, d_out);
     SBWT_CHECK_CUDA(cudaGetLastError());
     return 0;
 }

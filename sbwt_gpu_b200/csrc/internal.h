@@ -56,6 +56,9 @@ struct SearchArgs {
     u64 bloom_mask;
     u32 bloom_hashes;
     unsigned long long *skipped;
+    // run walk of a batch of reads behind the learned prefilter: bit j%32 of
+    // word j/32 = k-mer j rejected by the model and the backup Bloom filter
+    const uint32_t *reject;
 };
 
 struct KernelShape {
@@ -67,6 +70,10 @@ struct KernelShape {
     int kind = SBWT_POPPY;
     int shuffles = 0;
     int mode = SBWT_SEARCH_STREAM;  // batches of reads with the queue-fed form (sbwt_params.search_mode)
+    // knobs of the run walk (batches of reads), set by the autotuner:
+    u32 window = 128;        // k-mers per window (line layout: 64, 128 or 256)
+    u32 blocks_per_sm = 0;   // resident blocks per SM of the persistent grid (0: as many as fit)
+    int evict = 0;           // evict-first gathers: 0 = when a table exceeds half of L2, 1 = never, 2 = always
 };
 
 // Device buffers of one in-flight search (grow-only).
@@ -114,6 +121,9 @@ struct sbwt_index {
     ulonglong4 *d_lines = nullptr;
     uint32_t lpc = 0;
     bool lines_ok = false;
+    // wide lines (SBWT_LAYOUT_LINES512 / LINES2048): wide_s sectors per line, 0 = not built
+    ulonglong4 *d_wide = nullptr;
+    uint32_t wide_s = 0, wide_lpc = 0;
     // POPPY layout
     uint64_t *d_L0 = nullptr, *d_L12 = nullptr;
     uint64_t l0w = 0, l12w = 0;
@@ -128,6 +138,7 @@ struct sbwt_index {
     // the entry up in d_pre, the interval is wider than the field holds)
     uint32_t *d_pre32 = nullptr;
     bool pre64 = false;
+    int compact_pre = -1;  // the compact table: -1 = from SBWT_PRESEARCH_COMPACT, 0 = off, 1 = on
     // backward-step structures (stream.cu): node nibbles, select samples, backward table
     uint8_t *d_node = nullptr;
     uint32_t *d_sel = nullptr;
@@ -163,6 +174,11 @@ namespace sbwt {
 // rank_build.cu
 int build_lines(sbwt_index *ix, cudaStream_t s, uint64_t ones[4]);
 int build_poppy(sbwt_index *ix, uint32_t sb, int kind, cudaStream_t s);
+// The wide-line layout of `sectors` (2 or 8) 32-byte sectors per line.
+int build_wide(sbwt_index *ix, uint32_t sectors, cudaStream_t s);
+inline uint32_t wide_sectors(int layout) {
+    return layout == SBWT_LAYOUT_LINES512 ? 2u : layout == SBWT_LAYOUT_LINES2048 ? 8u : 0u;
+}
 int ensure_scan_scratch(sbwt_index *ix, uint64_t n_items);
 
 // presearch.cu
@@ -177,6 +193,9 @@ uint64_t scan_scratch_words(uint64_t n_items);
 int launch_chunk_rows(const uint64_t *d_kstart, uint64_t n_rows, uint64_t n_kmers, uint32_t chunk,
                       uint32_t *d_chunk_row, cudaStream_t s);
 int launch_member_bits(const uint64_t *d_answers, uint64_t n, uint32_t *d_bits, cudaStream_t s);
+// The k-mers j0 .. j0+count-1 of the batch of reads described by a (words,
+// row_starts, kstart, chunk_row, chunk, max_pos) as a list of 64-bit windows.
+int launch_kmer_list(const SearchArgs &a, uint64_t j0, uint64_t count, uint64_t *d_out, cudaStream_t s);
 
 // stream.cu
 int build_stream(sbwt_index *ix, cudaStream_t s);
@@ -186,6 +205,13 @@ dev::StreamView stream_view(const sbwt_index *ix);
 int packed_runs(Workspace &w, const u64 *positions, u64 n_kmers, u32 chunk, cudaStream_t s, u64 *n_rows);
 
 // api.cu
+// Launch arguments of a search with the index's current shape and mode (the
+// batch pointers left NULL); `rows`: a batch of reads.
+SearchArgs base_args(const sbwt_index *ix, bool rows);
+// Grows w for a batch of reads and enqueues pack -> per-row k-mer table ->
+// chunk table on s; fills the batch fields of a (a.chunk set by base_args).
+int prepare_rows(sbwt_index *ix, Workspace &w, SearchArgs &a, const uint8_t *d_letters, uint64_t n_letters,
+                 const uint64_t *d_rows, uint64_t n_rows, uint64_t n_kmers, cudaStream_t s);
 int search_rows_device(sbwt_index *ix, Workspace &w, const uint8_t *d_letters, u64 n_letters, const u64 *d_rows,
                        u64 n_rows, u64 *d_answers, uint32_t *d_member, u64 n_kmers, cudaStream_t s);
 template <class T> int grow(T *&p, size_t &cap, size_t need);

@@ -133,7 +133,7 @@ constexpr u32 kGroupCols = kHid / kColGroups;       // 64
 __global__ void __launch_bounds__(kInferThreads, 1)
     mlp_infer_kernel(const u64 *__restrict__ kmers, u64 n, u32 k, const bf16 *__restrict__ W1b,
                      const bf16 *__restrict__ W2b, const float *__restrict__ b1, const float *__restrict__ b2,
-                     const float *__restrict__ w3, const float *__restrict__ b3, float *__restrict__ logits, int *err) {
+                     const float *__restrict__ w3, const float *__restrict__ b3, const InferOut out, int *err) {
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ uint64_t bar;
     __shared__ u32 tmem_s;
@@ -167,14 +167,14 @@ __global__ void __launch_bounds__(kInferThreads, 1)
     const float bias3 = __ldg(b3);
     u32 phase = 0;
     bool ok = true;
+    // one-hot tile: thread (row tid % 128, chunk group tid / 128); the k-mer of
+    // the next tile is loaded while this tile's layer-1 MMA runs
+    const u32 xr = tid & (kTileM - 1u), xg = tid / kTileM;
+    u64 kmer = (u64)blockIdx.x * kTileM + xr < n ? kmers[(u64)blockIdx.x * kTileM + xr] : 0ull;
     for (u64 tile = blockIdx.x; ok && tile * kTileM < n; tile += gridDim.x) {
         {
-            // one-hot tile: thread (row tid % 128, chunk group tid / 128)
-            const u32 r = tid & (kTileM - 1u), g = tid / kTileM;
-            const u64 row = tile * kTileM + r;
-            const u64 kmer = row < n ? kmers[row] : 0ull;
             constexpr u32 kChunks = kIn / 8 / kColGroups;  // 4 of the 16 chunks of a row
-            onehot_chunks(sX, kTileM, r, kmer, k, g * kChunks, (g + 1) * kChunks);
+            onehot_chunks(sX, kTileM, xr, kmer, k, xg * kChunks, (xg + 1) * kChunks);
         }
         fence_smem_to_async();
         __syncthreads();
@@ -187,6 +187,10 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                 mma_ss(tD, da, db, idesc_bf16(kTileM, kHid), s > 0);
             }
             mma_commit(&bar);
+        }
+        {
+            const u64 nrow = (tile + gridDim.x) * kTileM + xr;
+            kmer = nrow < n ? kmers[nrow] : 0ull;
         }
         bool got = mbar_wait(&bar, phase, err, kErrInferWait1);
         phase ^= 1u;
@@ -259,7 +263,16 @@ __global__ void __launch_bounds__(kInferThreads, 1)
             float sum = 0.0f;
 #pragma unroll
             for (u32 g = 0; g < kColGroups; g++) sum += sRed[g * kTileM + trow];
-            if (row < n) logits[row] = sum + bias3;
+            const float lg = sum + bias3;
+            if (out.logits && row < n) out.logits[row] = lg;
+            if (out.reject) {
+                // the sandwich's decision: rejected by the model at tau and by the backup Bloom filter
+                const Bloom bloom{out.bloom_bits, out.bloom_mask, out.bloom_hashes};
+                const bool rej = row < n && lg < out.tau && !bloom.probe(kmer_key(kmers[row], k));
+                const u32 bits = __ballot_sync(0xffffffffu, rej);
+                const u64 first = tile * kTileM + quarter * 32u;  // this warp's 32 rows
+                if (lane == 0 && first < n) out.reject[first >> 5] = bits;
+            }
         }
         fence_before_sync();
         __syncthreads();
@@ -571,19 +584,23 @@ int gemm_tn(const bf16 *A, const bf16 *B, float *D, u32 M, u32 N, u32 K, u32 spl
 }
 
 int infer(const u64 *kmers, u64 n, u32 k, const bf16 *W1b, const bf16 *W2b, const float *theta, const MlpOffsets &off,
-          float *logits, int *err, int num_sms, cudaStream_t s) {
+          const InferOut &out, int *err, int num_sms, cudaStream_t s) {
     if (n == 0) return 0;
-    static bool attr_set = false;
-    if (!attr_set) {
+    // the shared-memory opt-in is a per-device function attribute
+    int dev = 0;
+    SBWT_CHECK_CUDA(cudaGetDevice(&dev));
+    static bool attr_set[kMaxDevicesAttr] = {};
+    if (dev < 0 || dev >= kMaxDevicesAttr) return set_error("device %d out of range", dev);
+    if (!attr_set[dev]) {
         SBWT_CHECK_CUDA(cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem));
-        attr_set = true;
+        attr_set[dev] = true;
     }
     for (const float *q : {theta + off.b1, theta + off.b2, theta + off.w3})
         if ((uintptr_t)q & 15u) return set_error("MLP parameters must be 16-byte aligned");
     const u64 tiles = (n + kTileM - 1) / kTileM;
     const u32 grid = (u32)std::min<u64>(tiles, (u64)num_sms);
     mlp_infer_kernel<<<grid, kInferThreads, kInferSmem, s>>>(kmers, n, k, W1b, W2b, theta + off.b1, theta + off.b2,
-                                                   theta + off.w3, theta + off.b3, logits, err);
+                                                   theta + off.w3, theta + off.b3, out, err);
     SBWT_CHECK_CUDA(cudaGetLastError());
     return 0;
 }

@@ -50,8 +50,22 @@ __global__ void accuracy_kernel(const float *logits, const uint8_t *labels, uint
 
 int gemm_tn(const __nv_bfloat16 *A, const __nv_bfloat16 *B, float *D, uint32_t M, uint32_t N, uint32_t K,
             uint32_t splits, int *err, cudaStream_t s);
+// Outputs of an inference pass: the logits (NULL: not written) and/or the
+// sandwich's reject bitmap (bit j%32 of word j/32 = k-mer j rejected by the
+// model at tau and by the backup Bloom filter; NULL: not written).
+struct InferOut {
+    float *logits;
+    uint32_t *reject;
+    float tau;
+    const uint32_t *bloom_bits;
+    uint64_t bloom_mask;
+    uint32_t bloom_hashes;
+};
+constexpr int kMaxDevicesAttr = 64;
+inline InferOut logits_only(float *logits) { return InferOut{logits, nullptr, 0.0f, nullptr, 0, 0}; }
+
 int infer(const uint64_t *kmers, uint64_t n, uint32_t k, const __nv_bfloat16 *W1b, const __nv_bfloat16 *W2b,
-          const float *theta, const MlpOffsets &off, float *logits, int *err, int num_sms, cudaStream_t s);
+          const float *theta, const MlpOffsets &off, const InferOut &out, int *err, int num_sms, cudaStream_t s);
 int transpose(const __nv_bfloat16 *src, __nv_bfloat16 *dst, uint32_t R, uint32_t C, cudaStream_t s);
 
 }  // namespace mlp

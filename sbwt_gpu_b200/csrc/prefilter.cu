@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -41,6 +42,12 @@ struct sbwt_prefilter {
     float *d_logits = nullptr;
     size_t logits_cap = 0;
     unsigned long long *d_skipped = nullptr;
+    // prefiltered searches of reads: the reject bitmap of the batch and a
+    // chunk of its k-mers as a list (the inference input)
+    uint32_t *d_reject = nullptr;
+    size_t reject_cap = 0;
+    uint64_t *d_klist = nullptr;
+    size_t klist_cap = 0;
     sbwt_prefilter_stats stats{};
 };
 
@@ -199,21 +206,7 @@ int search_list(sbwt_index *ix, const uint64_t *d_kmers, uint64_t n, uint64_t *d
     if (n == 0) return 0;
     Workspace &w = ix->ws[0];
     SBWT_TRY(grow(w.counter, w.counter_cap, 1));
-    SearchArgs a;
-    std::memset(&a, 0, sizeof(a));
-    a.lines = ix->d_lines;
-    a.lpc = ix->lpc;
-    a.bits = ix->d_bits;
-    a.L0 = ix->d_L0;
-    a.L12 = ix->d_L12;
-    a.wpv = ix->wpv;
-    a.l0w = ix->l0w;
-    a.l12w = ix->l12w;
-    std::memcpy(a.C, ix->C, sizeof(a.C));
-    a.pre = ix->d_pre;
-    a.p = ix->p;
-    a.k = ix->k;
-    a.chunk = search_chunk(ix, false);
+    SearchArgs a = base_args(ix, false);
     a.kmer_list = d_kmers;
     a.answers = d_answers;
     a.n_kmers = n;
@@ -341,7 +334,7 @@ extern "C" int sbwt_prefilter_train(sbwt_index *ix, const sbwt_mlp_params *prm, 
             const uint64_t na = std::min<uint64_t>(n_train, 4u << 20);
             float *lg = nullptr;
             SBWT_CHECK_CUDA(cudaMalloc(&lg, na * sizeof(float)));
-            rc = infer(d_train, na, ix->k, pf->W1b, pf->W2b, pf->theta, pf->off, lg, pf->d_err, ix->num_sms, s);
+            rc = infer(d_train, na, ix->k, pf->W1b, pf->W2b, pf->theta, pf->off, logits_only(lg), pf->d_err, ix->num_sms, s);
             if (rc == 0) {
                 accuracy_kernel<<<(unsigned)((na + 255) / 256), 256, 0, s>>>(lg, d_labels, na, pf->tau, d_cnt + 1);
                 unsigned long long cnt[2];
@@ -360,7 +353,7 @@ extern "C" int sbwt_prefilter_train(sbwt_index *ix, const sbwt_mlp_params *prm, 
         SBWT_CHECK_CUDA(cudaMalloc(&lg, nodes * sizeof(float)));
         enumerate_kernel<<<(unsigned)((nodes + 255) / 256), 256, 0, s>>>(ix->d_lines, ix->lpc, c5, (uint32_t)ix->n,
                                                                          ix->k, d_all);
-        rc = infer(d_all, nodes, ix->k, pf->W1b, pf->W2b, pf->theta, pf->off, lg, pf->d_err, ix->num_sms, s);
+        rc = infer(d_all, nodes, ix->k, pf->W1b, pf->W2b, pf->theta, pf->off, logits_only(lg), pf->d_err, ix->num_sms, s);
         if (rc == 0) {
             cudaMemsetAsync(d_cnt + 2, 0, sizeof(unsigned long long), s);
             bloom_build_kernel<<<(unsigned)((nodes + 255) / 256), 256, 0, s>>>(d_all, lg, nodes, pf->tau, ix->k,
@@ -429,6 +422,8 @@ extern "C" void sbwt_prefilter_free(sbwt_prefilter *pf) {
     cudaFree(pf->W1b);
     cudaFree(pf->W2b);
     cudaFree(pf->bloom);
+    cudaFree(pf->d_reject);
+    cudaFree(pf->d_klist);
     cudaFree(pf->d_err);
     cudaFree(pf->d_logits);
     cudaFree(pf->d_skipped);
@@ -459,7 +454,7 @@ extern "C" int sbwt_prefilter_logits(sbwt_prefilter *pf, const uint64_t *d_kmers
     SBWT_CHECK_CUDA(cudaSetDevice(pf->device));
     int dev_sms = 0;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, pf->device);
-    return infer(d_kmers, n, pf->k, pf->W1b, pf->W2b, pf->theta, pf->off, d_logits, pf->d_err, dev_sms,
+    return infer(d_kmers, n, pf->k, pf->W1b, pf->W2b, pf->theta, pf->off, logits_only(d_logits), pf->d_err, dev_sms,
                  (cudaStream_t)stream);
 }
 
@@ -491,9 +486,74 @@ extern "C" int sbwt_search_kmers_filtered(sbwt_index *ix, sbwt_prefilter *pf, co
         SBWT_CHECK_CUDA(cudaMalloc(&pf->d_logits, n * sizeof(float)));
         pf->logits_cap = n;
     }
-    SBWT_TRY(infer(d_kmers, n, pf->k, pf->W1b, pf->W2b, pf->theta, pf->off, pf->d_logits, pf->d_err, ix->num_sms, s));
+    SBWT_TRY(infer(d_kmers, n, pf->k, pf->W1b, pf->W2b, pf->theta, pf->off, logits_only(pf->d_logits), pf->d_err,
+                   ix->num_sms, s));
     SBWT_CHECK_CUDA(cudaMemsetAsync(pf->d_skipped, 0, sizeof(unsigned long long), s));
     SBWT_TRY(search_list(ix, d_kmers, n, d_answers, pf->d_logits, pf, pf->d_skipped, s));
+    if (n_skipped) {
+        unsigned long long c = 0;
+        SBWT_CHECK_CUDA(cudaMemcpyAsync(&c, pf->d_skipped, sizeof(c), cudaMemcpyDeviceToHost, s));
+        SBWT_CHECK_CUDA(cudaStreamSynchronize(s));
+        *n_skipped = c;
+        int e = 0;
+        SBWT_CHECK_CUDA(cudaMemcpy(&e, pf->d_err, sizeof(e), cudaMemcpyDeviceToHost));
+        if (e) return set_error("prefilter inference: a tensor-core wait timed out (code %d)", e);
+    }
+    return 0;
+}
+
+namespace {
+// k-mers per inference pass of a prefiltered search of reads (the list is
+// 8 bytes a k-mer); a multiple of the 128-k-mer tile.  Environment:
+// SBWT_FILTER_CHUNK_KMERS sets another size (rounded up to 128).
+uint64_t filter_chunk() {
+    uint64_t c = 64ull << 20;
+    if (const char *e = std::getenv("SBWT_FILTER_CHUNK_KMERS")) {
+        const unsigned long long v = std::strtoull(e, nullptr, 10);
+        if (v) c = (v + 127) / 128 * 128;
+    }
+    return c;
+}
+}  // namespace
+
+extern "C" int sbwt_search_reads_filtered(sbwt_index *ix, sbwt_prefilter *pf, const uint8_t *d_letters,
+                                          uint64_t n_letters, const uint64_t *d_row_starts, uint64_t n_rows,
+                                          uint64_t *d_answers, uint32_t *d_member_bits, uint64_t n_kmers,
+                                          uint64_t *n_skipped, void *stream) {
+    clear_error();
+    if (!ix || !pf) return set_error("NULL argument");
+    if (pf->k != ix->k) return set_error("the prefilter was trained for k = %u", pf->k);
+    if (n_skipped) *n_skipped = 0;
+    if (n_rows == 0 || n_kmers == 0) return 0;
+    if (!d_letters || !d_row_starts) return set_error("NULL device pointer");
+    if (!d_answers && !d_member_bits) return set_error("NULL answers and membership pointers");
+    SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    Workspace &w = ix->ws[0];
+    SearchArgs a = base_args(ix, true);
+    if (!a.runs || ix->shape.layout != SBWT_LAYOUT_LINES)
+        return set_error("the prefiltered search of reads needs the run walk on the line layout "
+                         "(search mode stream or skip, one lane per k-mer, queue-fed)");
+    SBWT_TRY(prepare_rows(ix, w, a, d_letters, n_letters, d_row_starts, n_rows, n_kmers, s));
+    const uint64_t words = (n_kmers + 31) / 32;
+    SBWT_TRY(grow(pf->d_reject, pf->reject_cap, words));
+    const uint64_t chunk = filter_chunk();
+    SBWT_TRY(grow(pf->d_klist, pf->klist_cap, std::min(n_kmers, chunk)));
+    // the sandwich's decision for every k-mer of the batch: model at tau, then the backup Bloom filter
+    const InferOut out{nullptr, nullptr, pf->tau, pf->bloom, pf->bloom_mask, pf->bloom_hashes};
+    for (uint64_t j0 = 0; j0 < n_kmers; j0 += chunk) {
+        const uint64_t cnt = std::min(chunk, n_kmers - j0);
+        SBWT_TRY(launch_kmer_list(a, j0, cnt, pf->d_klist, s));
+        InferOut o = out;
+        o.reject = pf->d_reject + j0 / 32;
+        SBWT_TRY(infer(pf->d_klist, cnt, pf->k, pf->W1b, pf->W2b, pf->theta, pf->off, o, pf->d_err, ix->num_sms, s));
+    }
+    SBWT_CHECK_CUDA(cudaMemsetAsync(pf->d_skipped, 0, sizeof(unsigned long long), s));
+    a.reject = pf->d_reject;
+    a.skipped = pf->d_skipped;
+    a.answers = d_answers;
+    a.member = d_member_bits;
+    SBWT_TRY(launch_search(ix, a, s, nullptr));
     if (n_skipped) {
         unsigned long long c = 0;
         SBWT_CHECK_CUDA(cudaMemcpyAsync(&c, pf->d_skipped, sizeof(c), cudaMemcpyDeviceToHost, s));
@@ -559,7 +619,7 @@ extern "C" int sbwt_mlp_logits(uint32_t k, const float *theta, const uint64_t *k
         to_bf16_kernel<<<(256 * 256 + 255) / 256, 256>>>(d_th + off.W2, w2, 256 * 256);
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
-        rc = infer(d_k, n, k, w1, w2, d_th, off, d_lg, err, sms, 0);
+        rc = infer(d_k, n, k, w1, w2, d_th, off, logits_only(d_lg), err, sms, 0);
         if (rc == 0) {
             cudaError_t e = cudaDeviceSynchronize();
             if (e != cudaSuccess) rc = set_error("inference failed: %s", cudaGetErrorString(e));

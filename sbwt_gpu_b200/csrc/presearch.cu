@@ -94,14 +94,17 @@ __global__ void pre_compact_kernel(const uint2 *__restrict__ pre, u64 count, uin
     }
 }
 
-// The compact table of the run walk is built when the environment variable
-// SBWT_PRESEARCH_COMPACT is "1" and the index is small enough for it.
+// The compact table of the run walk is built when the index is small enough
+// for it and the autotuner chose it, or (no choice made) the environment
+// variable SBWT_PRESEARCH_COMPACT is "1".
 // Measured on the large workload (p = 12, 100.2M columns): 8.375 ms per
 // search against 8.317 ms with the 8-byte entries alone, so it is off by
 // default.
 bool compact_presearch(const sbwt_index *ix) {
+    if (ix->n >= dev::kPreMaxColumns) return false;
+    if (ix->compact_pre >= 0) return ix->compact_pre == 1;  // the autotuner's choice
     const char *e = std::getenv("SBWT_PRESEARCH_COMPACT");
-    return ix->n < dev::kPreMaxColumns && e && e[0] == '1' && e[1] == 0;
+    return e && e[0] == '1' && e[1] == 0;
 }
 
 }  // namespace

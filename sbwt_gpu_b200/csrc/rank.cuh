@@ -107,6 +107,60 @@ struct LinesRankerT {
 };
 using LinesRanker = LinesRankerT<1>;
 
+// ------------------------------------------------------------- WIDE lines
+
+template <int S>
+struct WideRanker {
+    using IT = u32;
+    using Sh = WideShape<S>;
+    const ulonglong4 *lines;  // vector c's line j at lines + (c * lpc + j) * S
+    u32 lpc;
+
+    // Per rank: the header sector of its line and the sector holding its bit
+    // (the header again when that is sector 0).  A single-node interval
+    // (l == r) needs one rank: rank(r+1) = rank(l) + bit(l).
+    struct Fetch {
+        ulonglong4 ha, xa, hb, xb;
+        u32 qa, qb;
+        bool single;
+    };
+
+    __device__ __forceinline__ void load(const ulonglong4 *base, u32 x, u32 &q, ulonglong4 &h, ulonglong4 &d) const {
+        const u32 line = x / Sh::kDataBits;
+        q = x - line * Sh::kDataBits;
+        const ulonglong4 *ln = base + (u64)line * S;
+        const u32 sec = (Sh::kHeaderBits + q) >> 8;
+        h = ld_line(ln);
+        d = sec ? ld_line(ln + sec) : h;
+    }
+
+    __device__ __forceinline__ Fetch fetch(u32 c, u32 l, u32 r, u32) const {
+        Fetch f;
+        const ulonglong4 *base = lines + (u64)c * lpc * S;
+        f.single = l == r;
+        load(base, l, f.qa, f.ha, f.xa);
+        if (!f.single) load(base, r + 1u, f.qb, f.hb, f.xb);
+        return f;
+    }
+
+    __device__ __forceinline__ void finish(const Fetch &f, u32 Cc, u32 &l, u32 &r, u32, u32) const {
+        u32 bit;
+        const u32 ra = wide_rank<S>(f.ha, f.xa, f.qa, bit);
+        l = Cc + ra;
+        if (f.single) {
+            r = Cc + ra + bit - 1u;
+        } else {
+            u32 bb;
+            r = Cc + wide_rank<S>(f.hb, f.xb, f.qb, bb) - 1u;
+        }
+    }
+
+    __device__ __forceinline__ void step(u32 c, u32 Cc, u32 &l, u32 &r) const {
+        const Fetch f = fetch(c, l, r, 0);
+        finish(f, Cc, l, r, 0, 0xffffffffu);
+    }
+};
+
 // ------------------------------------------------------------------ POPPY
 
 template <int SB, int KIND, class ITT, int TPK = 1>

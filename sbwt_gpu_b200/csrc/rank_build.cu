@@ -58,6 +58,60 @@ struct LinesBuild {
     }
 };
 
+// ------------------------------------------------------------- wide lines
+
+// Line li of a wide layout (device.cuh WideShape): the scan value is the
+// line's ones; emit reassembles its data bits from the raw vector, adds the
+// per-sector counts and writes the S sectors.
+template <int S>
+struct WideBuild {
+    using Sh = WideShape<S>;
+    static constexpr u32 kWords = 4u * S;
+    const u64 *src;  // one vector, reference word layout
+    u64 wsrc;        // readable words
+    ulonglong4 *dst;
+    struct Item {
+        u32 ones;
+    };
+    __device__ __forceinline__ u64 word(u64 wi) const { return wi < wsrc ? src[wi] : 0ull; }
+    // 64 source bits starting at bit position P (MSB-first)
+    __device__ __forceinline__ u64 bits64(u64 P) const {
+        const u64 wi = P >> 6;
+        const u32 off = (u32)(P & 63u);
+        const u64 a = word(wi);
+        return off ? (a << off) | (word(wi + 1) >> (64u - off)) : a;
+    }
+    // line word i's data bits (header bits zero)
+    __device__ __forceinline__ u64 data_word(u64 li, u32 i) const {
+        constexpr u32 H = Sh::kHeaderBits;
+        const u64 P0 = li * Sh::kDataBits;
+        if (64u * (i + 1) <= H) return 0ull;
+        if (64u * i < H) return bits64(P0) >> (H - 64u * i);
+        return bits64(P0 + (64u * i - H));  // the data bits end with the line (H + D = 256 S)
+    }
+    __device__ __forceinline__ Item load(u64 li) const {
+        u32 c = 0;
+#pragma unroll 4
+        for (u32 i = 0; i < kWords; i++) c += __popcll(data_word(li, i));
+        return Item{c};
+    }
+    __device__ __forceinline__ u64 value(const Item &it) const { return it.ones; }
+    __device__ __forceinline__ void emit(u64 li, u64 prefix, const Item &) const {
+        u64 *out = reinterpret_cast<u64 *>(dst + li * S);
+        u64 head[3] = {prefix << 32, 0ull, 0ull};  // the header lies in line words 0..2
+        u32 run = 0;                               // ones in the sectors before the current one
+#pragma unroll 1
+        for (u32 sec = 0; sec < (u32)S; sec++) {
+            if (sec) {  // sub[sec] = ones of the data bits in sectors 0..sec-1, 16 bits at line bit 32 + 16 (sec-1)
+                const u32 b0 = 32u + 16u * (sec - 1u);
+                head[b0 >> 6] |= (u64)run << (48u - (b0 & 63u));
+            }
+            for (u32 i = 4u * sec; i < 4u * sec + 4u; i++) run += __popcll(data_word(li, i));
+        }
+        for (u32 i = 0; i < kWords; i++) out[i] = data_word(li, i) | (i < 3 ? head[i] : 0ull);
+    }
+};
+
 // ------------------------------------------------------------------ POPPY
 
 template <int SB, int KIND>
@@ -190,6 +244,45 @@ int build_lines(sbwt_index *ix, cudaStream_t s, uint64_t ones[4]) {
     }
     cudaFree(totals);
     return rc;
+}
+
+template <int S>
+int wide_all(sbwt_index *ix, cudaStream_t s) {
+    const u64 nl = ix->wide_lpc;
+    SBWT_TRY(ensure_scan_scratch(ix, nl));
+    u64 *totals = nullptr;
+    SBWT_CHECK_CUDA(cudaMalloc(&totals, 4 * sizeof(u64)));
+    int rc = 0;
+    for (int c = 0; c < 4 && rc == 0; c++) {
+        WideBuild<S> f;
+        f.src = ix->d_bits + (u64)c * ix->wpv;
+        f.wsrc = ix->wpv;
+        f.dst = ix->d_wide + (u64)c * nl * S;
+        cudaError_t e = device_scan(f, nl, ix->d_scan, totals + c, s);
+        if (e != cudaSuccess) rc = set_error("wide line build launch failed: %s", cudaGetErrorString(e));
+    }
+    if (rc == 0) {
+        const cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = set_error("wide line build failed: %s", cudaGetErrorString(e));
+    }
+    cudaFree(totals);
+    return rc;
+}
+
+int build_wide(sbwt_index *ix, uint32_t sectors, cudaStream_t s) {
+    if (sectors != 2 && sectors != 8) return set_error("wide lines have 2 or 8 sectors (got %u)", sectors);
+    const u64 data = sectors == 2 ? WideShape<2>::kDataBits : WideShape<8>::kDataBits;
+    const u64 nl = (ix->n / data + 1 + 7) / 8 * 8;
+    if (ix->n >= (1ull << 32) || nl > 0xffffffffull) return set_error("wide lines serve indexes below 2^32 columns");
+    ix->gen++;
+    if (ix->d_wide) cudaFree(ix->d_wide);
+    ix->d_wide = nullptr;
+    ix->wide_s = 0;
+    SBWT_CHECK_CUDA(cudaMalloc(&ix->d_wide, 4ull * nl * sectors * sizeof(ulonglong4)));
+    ix->wide_lpc = (u32)nl;
+    SBWT_TRY(sectors == 2 ? wide_all<2>(ix, s) : wide_all<8>(ix, s));
+    ix->wide_s = sectors;
+    return 0;
 }
 
 int build_poppy(sbwt_index *ix, uint32_t sb, int kind, cudaStream_t s) {

@@ -24,6 +24,7 @@
 // (sbwt_search_packed) or through a per-row table (sbwt_search_reads): no
 // positions array is materialised there.
 #include <algorithm>
+#include <type_traits>
 
 #include "device.cuh"
 #include "internal.h"
@@ -339,8 +340,8 @@ __global__ void __launch_bounds__(128) search_queue_kernel(const R rk, const Sea
 // k-mers starting at j+m-k .. j are all absent.  An empty presearch entry
 // gives m = p.  This kernel walks each run of k-mers of one row from right
 // to left and, after a search that fails at m letters, moves left by k-m+1
-// k-mers at once.  Their answers are the ~0 written when the run's window
-// was taken, so every answer equals the reference's per-k-mer search.
+// k-mers at once and answers ~0 for all of them, so every answer equals the
+// reference's per-k-mer search.
 //
 // With STREAM, a found k-mer's node also gives the node of the k-mer one
 // letter to its left by one backward step (stream.cuh) instead of a search
@@ -348,8 +349,8 @@ __global__ void __launch_bounds__(128) search_queue_kernel(const R rk, const Sea
 // k-mer is absent, and the next one is searched again.
 //
 // Work split: a warp takes 32 windows of kWin consecutive k-mer indices from
-// the global cursor and writes ~0 to all their answers (coalesced), and zero
-// to their membership words.  Each lane cuts its window at row ends into runs
+// the global cursor and writes zero to their membership words (coalesced).
+// Each lane cuts its window at row ends into runs
 // and enqueues one run per fill into the warp's shared-memory queue; an idle
 // lane pops a run.  Every loop iteration a lane either starts its run's next
 // k-mer (backward step, or letters + presearch entry followed by its first
@@ -359,18 +360,84 @@ __global__ void __launch_bounds__(128) search_queue_kernel(const R rk, const Sea
 // the longest run).  Longer runs mean fewer fresh searches per read (one per
 // run start, plus one per absent stretch) and a longer walk per lane.
 // Measured on the large, batched and pangenome workloads: 128 beats 32 by
-// 9-16 % (fewer run starts), 256 starts to lose to the longer tail.
-#ifndef SBWT_RUNS_WINDOW
-#define SBWT_RUNS_WINDOW 128
-#endif
-constexpr u32 kWin = SBWT_RUNS_WINDOW;
-static_assert(kWin % 32 == 0, "windows cover whole bitmap words");
+// 9-16 % (fewer run starts), 256 starts to lose to the longer tail.  The
+// line layout also serves 64 and 256 (KernelShape.window, set by the
+// autotuner); the other layouts use 128.
+constexpr u32 kWin = 128;
 
-// Answers: a warp writes ~0 to all answers of its windows when it takes them
-// (coalesced) and found k-mers overwrite theirs.  (Writing each answer once,
-// by the lane that settles it, was measured 22 % slower on the large
-// workload: the skip's bursts of single 8-byte stores cost more than the
-// rewritten sectors.)
+// Answers are written once, a 32-byte sector (4 answers) at a time.  A lane
+// settles its run's k-mers strictly right to left and without gaps, so it
+// stages the answers of the sector it is in (shared memory, 4 x u64 per
+// lane) and stores the sector with one 256-bit streaming store once its
+// lowest k-mer is settled; sectors that a long absent stretch covers whole
+// go out directly.  Only the sectors at the two ends of a run (row ends)
+// are stored answer by answer.  The stores carry the streaming (evict-first)
+// hint, so the answer stream does not push the index out of L2.  (The
+// previous form wrote ~0 over a warp's 32 windows when it took them and
+// overwrote the found answers later; the prefilled sectors had left L2 by
+// then, so each overwrite cost a DRAM read and a rewrite.)  Build option
+// SBWT_ANSWER_WRITE_ONCE=0 restores that form.
+#ifndef SBWT_ANSWER_WRITE_ONCE
+#define SBWT_ANSWER_WRITE_ONCE 1
+#endif
+
+#if SBWT_ANSWER_WRITE_ONCE
+__device__ __forceinline__ void st_stream4(u64 *p, u64 a, u64 b, u64 c, u64 d) {
+    asm volatile("st.global.cs.v4.u64 [%0], {%1, %2, %3, %4};" ::"l"(p), "l"(a), "l"(b), "l"(c), "l"(d) : "memory");
+}
+__device__ __forceinline__ void st_stream(u64 *p, u64 a) {
+    asm volatile("st.global.cs.u64 [%0], %1;" ::"l"(p), "l"(a) : "memory");
+}
+
+// One lane's staged sector, in shared memory: slot[0..3] and, in slot[4],
+// the last (rightmost) k-mer of the lane's current run.  Sector boundaries
+// are where the answer's address is a multiple of 32 bytes: k-mer x sits in
+// slot (x + aoff) & 3, aoff = (answers address / 8) mod 4.  The answer
+// pointer is read from the kernel parameters at each use, so the stage
+// costs the walk no registers.
+__device__ __forceinline__ u32 stage_slot(const u64 *ans, u64 x) {
+    return (u32)(x + (reinterpret_cast<uintptr_t>(ans) >> 3)) & 3u;
+}
+
+// Store the staged slots s .. top of the sector whose slot s holds k-mer x
+// (x is the lowest settled k-mer of that sector).
+__device__ __forceinline__ void stage_flush(u64 *ans, const u64 *slot, u64 x, u32 s) {
+    const u32 top = min(3u, s + (u32)min(slot[4] - x, (u64)3));
+    if (s == 0 && top == 3) {
+        const ulonglong2 v0 = *reinterpret_cast<const ulonglong2 *>(slot);
+        const ulonglong2 v1 = *reinterpret_cast<const ulonglong2 *>(slot + 2);
+        st_stream4(ans + x, v0.x, v0.y, v1.x, v1.y);
+    } else {
+        for (u32 t = s; t <= top; t++) st_stream(ans + (x - s + t), slot[t]);
+    }
+}
+
+// k-mer x found with node v; lo = the run's first k-mer.
+__device__ __forceinline__ void stage_found(u64 *ans, u64 *slot, u64 x, u64 v, u64 lo) {
+    const u32 s = stage_slot(ans, x);
+    slot[s] = v;
+    if (s == 0 || x == lo) stage_flush(ans, slot, x, s);
+}
+
+// k-mers b .. x absent (b >= lo, the run's first k-mer).
+__device__ __forceinline__ void stage_absent(u64 *ans, u64 *slot, u64 x, u64 b, u64 lo) {
+#pragma unroll 1
+    for (;;) {
+        const u32 s = stage_slot(ans, x);
+        const u64 a = x - min((u64)s, x - b);  // lowest k-mer of this sector in [b, x]
+        const u32 sa = s - (u32)(x - a);
+        if (sa == 0 && s == 3) {
+            st_stream4(ans + a, ~0ull, ~0ull, ~0ull, ~0ull);  // the whole sector
+        } else {
+            for (u32 t = sa; t <= s; t++) slot[t] = ~0ull;
+            if (sa == 0 || a == lo) stage_flush(ans, slot, a, sa);
+        }
+        if (a == b) break;
+        x = a - 1u;
+    }
+}
+
+#endif  // SBWT_ANSWER_WRITE_ONCE
 
 // Resident 128-thread blocks per SM the run-walking kernel is compiled for
 // (a register cap), measured on the large workload: 9 for the line ranker
@@ -379,6 +446,7 @@ static_assert(kWin % 32 == 0, "windows cover whole bitmap words");
 // the larger poppy blocks keep the compiler's choice (a cap spills there).
 template <class R> struct RunsMinBlocks { static constexpr int value = 1; };
 template <int TPK> struct RunsMinBlocks<LinesRankerT<TPK>> { static constexpr int value = 9; };
+template <int S> struct RunsMinBlocks<WideRanker<S>> { static constexpr int value = 8; };
 template <int SB, int KIND, class IT, int TPK> struct RunsMinBlocks<PoppyRanker<SB, KIND, IT, TPK>> {
     static constexpr int value = SB <= 1024 ? 10 : 1;
 };
@@ -387,13 +455,23 @@ constexpr u32 kStart = 0xfffffffeu; // lane state: start the run's current k-mer
 struct RunEntry {
     u64 pos;  // letter offset of the run's last (rightmost) k-mer
     u64 j;    // k-mer index of that k-mer
-    u32 len;  // k-mers in the run, 1..kWin
+    u32 len;  // k-mers in the run, 1..WIN
 };
 
-template <class R, bool STREAM>
+// FILTER: the learned prefilter's reject bitmap (a.reject) is read before
+// each search from scratch; a rejected k-mer is answered absent unsearched
+// (the learned-Bloom sandwich: rejected by the model and by the backup Bloom
+// filter over the indexed k-mers the model rejects, so never a present one),
+// and the walk goes on with the k-mer to its left.
+template <class R, bool STREAM, bool FILTER, u32 WIN>
 __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kernel(const R rk, const SearchArgs a) {
     static_assert(sizeof(typename R::IT) == 4, "the run form serves 32-bit intervals");
+    static_assert(WIN % 32 == 0, "windows cover whole bitmap words");
     __shared__ RunEntry queue[kQueueWarps][kQueue];
+#if SBWT_ANSWER_WRITE_ONCE
+    // per lane: 4 staged answers, the run's last k-mer, pending membership bits
+    __shared__ __align__(16) u64 staged[kQueueWarps * 32][6];
+#endif
     using PT = uint2;
     const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const u32 lt = (1u << lane) - 1u;
@@ -404,6 +482,10 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
     const u64 n_eff = min(a.n_kmers, a.kstart[a.n_rows]);
     uint32_t *const member = a.member;
     RunEntry *q = queue[warp];
+#if SBWT_ANSWER_WRITE_ONCE
+    u64 *const slot = staged[threadIdx.x];
+    slot[5] = 0;
+#endif
 
     u32 head = 0, tail = 0;  // warp-uniform
     bool more = true;
@@ -413,24 +495,27 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
     u32 L = 0, Rr = 0, I = kDone;
     u32 V = dev::kNoNode;          // STREAM: node of the k-mer right of J (found), or kNoNode
     const u64 gpol = l2_evict_first_policy();  // for the gathers from tables too large for L2
+    u32 n_skip = 0;                            // FILTER: k-mers answered from the reject bitmap
 
     for (;;) {
         // ---- fill: new windows once every lane's window is cut, then one run per lane
         if (more && tail - head < 32u) {
             if (__ballot_sync(kFull, pj < pe) == 0) {
                 unsigned long long base = 0;
-                if (lane == 0) base = atomicAdd(a.counter, (unsigned long long)(32u * kWin));
+                if (lane == 0) base = atomicAdd(a.counter, (unsigned long long)(32u * WIN));
                 base = __shfl_sync(kFull, base, 0);
                 if (base >= n_eff) {
                     more = false;
                 } else {
-                    const u64 end = min((u64)base + 32u * kWin, n_eff);
+                    const u64 end = min((u64)base + 32u * WIN, n_eff);
+#if !SBWT_ANSWER_WRITE_ONCE
                     if (a.answers)  // NULL: membership bitmap only
                         for (u64 t = base + lane; t < end; t += 32u) a.answers[t] = ~0ull;
-                    pj = min((u64)base + (u64)lane * kWin, end);
-                    pe = min(pj + kWin, end);
+#endif
+                    pj = min((u64)base + (u64)lane * WIN, end);
+                    pe = min(pj + WIN, end);
                     if (pj < pe) {
-                        prow = a.chunk_row[pj / kWin];
+                        prow = a.chunk_row[pj / WIN];
                         if (member)
                             for (u64 w = pj / 32u; w < (pe + 31u) / 32u; w++) member[w] = 0u;
                     }
@@ -468,6 +553,9 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
             left = e.len - 1u;
             I = kStart;
             V = dev::kNoNode;
+#if SBWT_ANSWER_WRITE_ONCE
+            slot[4] = e.j;
+#endif
         }
         head += take;
         __syncwarp();
@@ -480,6 +568,9 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
                 const u32 u = a.sv.back_step(V, letter, a.ef_back, gpol);
                 adv = 1;
                 if (u != dev::kNoNode) found = u;
+            } else if (FILTER && ((__ldg(a.reject + (J >> 5)) >> (J & 31u)) & 1u)) {
+                adv = 1;  // rejected by the prefilter: absent, unsearched
+                n_skip++;
             } else {
                 // ---- start: letters (search_kernel.hpp:66-68) and presearch entry (:71-82)
                 const u64 b = min(pos, a.max_pos) << 1;
@@ -529,10 +620,39 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
                 adv = 1;
             }
         }
+#if SBWT_ANSWER_WRITE_ONCE
+        if (adv) {
+            const u64 lo = J - left;  // the run's first k-mer
+            u32 &mword = *reinterpret_cast<u32 *>(slot + 5);  // found bits not yet or-ed into their word
+            if (found != ~0u) {
+                if (a.answers) stage_found(a.answers, slot, J, (u64)found, lo);
+                if (member) {
+                    const u32 m = mword | 1u << (J & 31u);
+                    if ((J & 31u) == 0 || J == lo) {
+                        atomicOr(member + (J >> 5), m);
+                        mword = 0;
+                    } else {
+                        mword = m;
+                    }
+                }
+            } else {
+                const u64 b = adv > left ? lo : J - (adv - 1u);  // k-mers b .. J are absent
+                if (a.answers) stage_absent(a.answers, slot, J, b, lo);
+                if (member && ((b >> 5) != (J >> 5) || (b & 31u) == 0 || b == lo)) {
+                    const u32 m = mword;
+                    if (m) {
+                        atomicOr(member + (J >> 5), m);
+                        mword = 0;
+                    }
+                }
+            }
+        }
+#else
         if (found != ~0u) {
             if (a.answers) a.answers[J] = (u64)found;
             if (member) atomicOr(member + (J >> 5), 1u << (J & 31u));
         }
+#endif
         if (adv) {
             if (STREAM) V = found != ~0u ? found : dev::kNoNode;
             if (adv > left) {
@@ -544,6 +664,10 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
                 I = kStart;
             }
         }
+    }
+    if (FILTER && a.skipped) {
+        for (u32 o = 16; o; o >>= 1) n_skip += __shfl_xor_sync(kFull, n_skip, o);
+        if (lane == 0 && n_skip) atomicAdd(a.skipped, (unsigned long long)n_skip);
     }
 }
 
@@ -563,13 +687,36 @@ int launch_one(const R &rk, SearchArgs &a, const sbwt_index *ix, cudaStream_t s,
     return 0;
 }
 
+template <class R, u32 WIN>
+auto runs_kernel(const SearchArgs &a) {
+    if constexpr (std::is_same<R, LinesRankerT<1>>::value) {  // the prefiltered walk: line layout only
+        if (a.reject) return a.stream ? search_runs_kernel<R, true, true, WIN> : search_runs_kernel<R, false, true, WIN>;
+    }
+    return a.stream ? search_runs_kernel<R, true, false, WIN> : search_runs_kernel<R, false, false, WIN>;
+}
+
 template <class R>
 int launch_queue(const R &rk, SearchArgs &a, const sbwt_index *ix, cudaStream_t s, u32 *blocks_out) {
-    auto kern = a.runs ? (a.stream ? search_runs_kernel<R, true> : search_runs_kernel<R, false>)
-                       : search_queue_kernel<R>;
+    auto kern = search_queue_kernel<R>;
+    if (a.runs) {
+        if constexpr (std::is_same<R, LinesRankerT<1>>::value) {
+            switch (a.chunk) {
+            case 64: kern = runs_kernel<R, 64>(a); break;
+            case 128: kern = runs_kernel<R, 128>(a); break;
+            case 256: kern = runs_kernel<R, 256>(a); break;
+            default: return set_error("window must be 64, 128 or 256 k-mers (got %u)", a.chunk);
+            }
+        } else {
+            if (a.chunk != kWin) return set_error("this layout walks windows of %u k-mers", kWin);
+            kern = runs_kernel<R, kWin>(a);
+        }
+    }
+    if (a.reject && (!a.runs || !std::is_same<R, LinesRankerT<1>>::value))
+        return set_error("the prefiltered search of reads needs the run walk on the line layout");
     int per_sm = 0;
     SBWT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, 0));
     if (per_sm < 1) per_sm = 1;
+    if (ix->shape.blocks_per_sm && (int)ix->shape.blocks_per_sm < per_sm) per_sm = (int)ix->shape.blocks_per_sm;
     const u32 blocks = (u32)per_sm * (u32)ix->num_sms;
     if (blocks_out) *blocks_out = blocks;
     SBWT_CHECK_CUDA(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), s));
@@ -594,6 +741,14 @@ int lines_kpt(const sbwt_index *ix, SearchArgs &a, cudaStream_t s, u32 kpt, u32 
     case 8: return launch_one<LinesRankerT<TPK>, 8, TPK>(rk, a, ix, s, tpb, blocks);
     default: return set_error("kmers_per_thread must be 1, 2, 3, 4, 6 or 8 (got %u)", kpt);
     }
+}
+
+template <int S>
+int wide_launch(const sbwt_index *ix, SearchArgs &a, cudaStream_t s, const KernelShape &sh, u32 *blocks) {
+    if (sh.kpt != 0 || sh.tpk != 1)
+        return set_error("the wide-line layouts serve the queue-fed kernels (kmers_per_thread 0, threads_per_kmer 1)");
+    WideRanker<S> rk{ix->d_wide, ix->wide_lpc};
+    return launch_queue(rk, a, ix, s, blocks);
 }
 
 template <int SB, int KIND, class IT, int TPK>
@@ -624,6 +779,7 @@ bool runs_form(const sbwt_index *ix) {
     const KernelShape &sh = ix->shape;
     if (sh.mode == SBWT_SEARCH_EVERY_KMER || sh.kpt != 0) return false;
     if (sh.layout == SBWT_LAYOUT_LINES) return ix->lines_ok && sh.tpk == 1;
+    if (wide_sectors(sh.layout)) return ix->wide_s == wide_sectors(sh.layout) && sh.tpk == 1;
     // poppy: the queue-fed forms are the 32-bit single-lane ones
     return ix->n < (1ull << 32) && !(sh.shuffles && (ix->sb == 1024 || ix->sb == 2048));
 }
@@ -634,7 +790,7 @@ bool stream_form(const sbwt_index *ix) {
 
 u32 search_chunk(const sbwt_index *ix, bool rows) {
     const KernelShape &sh = ix->shape;
-    if (rows && runs_form(ix)) return kWin;
+    if (rows && runs_form(ix)) return sh.layout == SBWT_LAYOUT_LINES && sh.window ? sh.window : kWin;
     const u32 groups = 32u / (sh.layout == SBWT_LAYOUT_LINES ? sh.tpk : 1u);
     if (sh.kpt == 0) return 32u * 16u;  // queue-fed form: 16 fills of 32 per chunk
     return groups * std::max(sh.kpt, 1u) * 8u;
@@ -643,6 +799,9 @@ u32 search_chunk(const sbwt_index *ix, bool rows) {
 int launch_search(const sbwt_index *ix, SearchArgs &a, cudaStream_t s, uint32_t *blocks) {
     const KernelShape &sh = ix->shape;
     if (a.n_kmers == 0) return 0;
+    if (a.reject && !(a.runs && sh.layout == SBWT_LAYOUT_LINES && sh.tpk == 1 && sh.kpt == 0))
+        return set_error("the prefiltered search of reads needs the run walk on the line layout "
+                         "(search mode stream or skip, one lane per k-mer, queue-fed)");
     if (sh.tpb == 0 || sh.tpb % 32 != 0 || sh.tpb > 256)
         return set_error("threads_per_block must be a multiple of 32 in [32, 256] (got %u)", sh.tpb);
     if (sh.layout == SBWT_LAYOUT_LINES) {
@@ -653,6 +812,10 @@ int launch_search(const sbwt_index *ix, SearchArgs &a, cudaStream_t s, uint32_t 
         case 4: return lines_kpt<4>(ix, a, s, sh.kpt, sh.tpb, blocks);
         default: return set_error("threads_per_kmer must be 1, 2 or 4 (got %u)", sh.tpk);
         }
+    }
+    if (wide_sectors(sh.layout)) {
+        if (ix->wide_s != wide_sectors(sh.layout)) return set_error("the wide-line layout has not been built");
+        return ix->wide_s == 2 ? wide_launch<2>(ix, a, s, sh, blocks) : wide_launch<8>(ix, a, s, sh, blocks);
     }
     if (!ix->poppy_ok) return set_error("the poppy layout has not been built");
     if (ix->kind == SBWT_POPPY) {

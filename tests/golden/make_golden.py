@@ -33,8 +33,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+from ref_program import REF_SEARCH, check_safe, reference_failed  # noqa: E402
+
 CASES = os.path.join(HERE, "cases")
-REF_SEARCH = os.path.join(ROOT, "oracle", "_ref", "search")
 
 # name: (seed, genome bp, reads, read length, k, p (0 = --without-presearch), SB, rank structure, shuffles)
 SPECS = {
@@ -85,16 +87,6 @@ def case_flags(name, cases=CASES):
     return flags
 
 
-def check_safe(n_bits, letters, rows, k, p):
-    lens = np.diff(rows.astype(np.int64))
-    n_kmers = int((lens - k + 1).sum())
-    assert (lens >= k).all(), "every read must be at least k long"
-    assert n_kmers % 64 == 0, "the k-mer count must be a multiple of 64"
-    assert n_bits % 4096 != 0, "n must not be a multiple of 4096"
-    assert p == 0 or 5 <= p <= 13
-    assert set(np.unique(letters).tolist()) <= set(b"ACGT")
-
-
 def prepare():
     import sbwt_gpu_b200 as sg
     from sbwt_gpu_b200 import workloads as wl
@@ -132,12 +124,6 @@ def run(out_dir):
             rc = subprocess.run([REF_SEARCH] + flags, stdout=fo, stderr=fe, env=env, timeout=300).returncode
         print(name, "rc", rc)
     shutil.rmtree(c1)
-
-
-def reference_failed(err):
-    """The reference's error reports (include/gpu/cuda.hpp:67-84, search_caller.hpp:68-71)."""
-    return (b"did not succeed" in err or re.search(rb"CUDA error \d+ \(", err) is not None
-            or re.search(rb"Last CUDA error code [1-9]", err) is not None)
 
 
 def collect(out_dir):

@@ -80,6 +80,27 @@ def test_presearch_table_matches_oracle(small, p):
     assert np.array_equal(rights, wr)
 
 
+@pytest.mark.parametrize("p", [13, 14])
+def test_deep_presearch_table_matches_oracle_on_a_sample(small, p):
+    """p = 13 and 14 (the depths the autotuner and the pangenome workload use): the whole GPU table is
+    exported; the oracle restates 2M sampled entries plus both ends of the table."""
+    b = small["built"]
+    ox = orc.OracleIndex(b.bits, b.n_bits)
+    with sg.Index.from_bits(b.bits, b.n_bits, k=31, k_presearch=p) as ix:
+        lefts, rights = ix.presearch_table()
+    n = 1 << (2 * p)
+    assert lefts.size == n and rights.size == n
+    rng = np.random.default_rng(p)
+    idx = np.concatenate([np.arange(1024, dtype=np.uint64), np.arange(n - 1024, n, dtype=np.uint64),
+                          rng.integers(0, n, size=2_000_000, dtype=np.uint64)])
+    wl_, wr = ox.presearch_at(p, idx)
+    assert np.array_equal(lefts[idx], wl_)
+    assert np.array_equal(rights[idx], wr)
+    # every non-empty entry lies inside the index
+    ne = lefts <= rights
+    assert ne.any() and int(rights[ne].max()) < b.n_bits
+
+
 def test_search_packed_reference_contract(small, cuda):
     b, k = small["built"], small["k"]
     ox = orc.OracleIndex(b.bits, b.n_bits)
@@ -367,7 +388,8 @@ def _row_mixture(rng, genome, k):
 
 
 @pytest.mark.parametrize("k,p", [(31, 10), (31, 0), (31, 13), (5, 3), (5, 5), (32, 12), (12, 6), (3, 2)])
-@pytest.mark.parametrize("layout", [sg.SBWT_LAYOUT_LINES, sg.SBWT_LAYOUT_POPPY])
+@pytest.mark.parametrize("layout", [sg.SBWT_LAYOUT_LINES, sg.SBWT_LAYOUT_POPPY, sg.SBWT_LAYOUT_LINES512,
+                                    sg.SBWT_LAYOUT_LINES2048])
 def test_run_walk_modes_equal_per_kmer_search(cuda, k, p, layout):
     """The right-to-left run walk (absent-run skip, and skip + backward steps) answers
     exactly as the per-k-mer search and the oracle, bitmap included."""

@@ -164,3 +164,75 @@ def test_trained_network_gains_over_the_untrained_one(trained, cuda):
     assert t["auc"] > 0.95 and t["auc"] > u["auc"] + 0.2, out
     assert t["rejected_indexed"] < 0.25 * u["rejected_indexed"], out
     assert t["skip"] > 0.3 and u["skip"] > 0, out
+
+
+def _concat_files(files):
+    letters = np.concatenate([lt for lt, _ in files])
+    rows, off = [np.zeros(1, dtype=np.uint64)], 0
+    for lt, rw in files:
+        rows.append(rw[1:].astype(np.uint64) + np.uint64(off))
+        off += lt.size
+    return letters, np.concatenate(rows)
+
+
+def _filtered_vs_oracle(ix, pf, built, letters, rows, k, p, cuda, monkeypatch=None, chunk=None):
+    import torch
+    if chunk is not None:
+        monkeypatch.setenv("SBWT_FILTER_CHUNK_KMERS", str(chunk))
+    nk = sg.count_kmers(rows, k)
+    d_l = torch.from_numpy(letters).to(cuda)
+    d_r = torch.from_numpy(rows.view(np.int64)).to(cuda)
+    filt = torch.full((nk,), -5, dtype=torch.int64, device=cuda)
+    bits = torch.full(((nk + 31) // 32,), -1, dtype=torch.int32, device=cuda)
+    skipped = ix.search_reads_filtered(pf, d_l, d_r, filt, nk, d_member_bits=bits)
+    only = torch.full(((nk + 31) // 32,), -1, dtype=torch.int32, device=cuda)  # membership only
+    ix.search_reads_filtered(pf, d_l, d_r, None, nk, d_member_bits=only)
+    torch.cuda.synchronize()
+    want = orc.OracleIndex(built.bits, built.n_bits).search_reads(letters, rows, k, p)
+    got = filt.cpu().numpy().view(np.uint64)
+    assert np.array_equal(got, want)  # bit-exact, so no indexed k-mer is reported absent
+    full = nk // 32
+    hit = np.zeros((nk + 31) // 32 * 32, dtype=bool)
+    hit[:nk] = want != orc.NOT_FOUND
+    want_bits = np.packbits(hit.reshape(-1, 32)[:, ::-1], axis=1).view(">u4").reshape(-1).astype(np.uint32)
+    assert np.array_equal(bits.cpu().numpy().view(np.uint32)[:full], want_bits[:full])
+    assert np.array_equal(only.cpu().numpy().view(np.uint32)[:full], want_bits[:full])
+    return skipped, nk, want
+
+
+def test_filtered_reads_batched_uneven_shape(trained, cuda, monkeypatch):
+    """The prefiltered search of reads (sbwt_search_reads_filtered) on the batched-uneven shape: 64 files of
+    150 bp / lognormal 2 kbp / lognormal 15 kbp reads, 30% genome reads with 2% substitutions, in one batch;
+    the inference runs in several chunks (a small chunk size), and the answers equal the oracle's."""
+    ix, pf, k = trained["ix"], trained["pf"], trained["k"]
+    files = list(wl.uneven_read_files(trained["genome"], seed=77, total_kmers=400_000, n_files=64))
+    letters, rows = _concat_files(files)
+    skipped, nk, want = _filtered_vs_oracle(ix, pf, trained["built"], letters, rows, k, 10, cuda, monkeypatch,
+                                            chunk=50_000)
+    assert 0 < skipped < nk
+    assert skipped <= int((want == orc.NOT_FOUND).sum())
+
+
+def test_filtered_reads_pangenome_shape(cuda):
+    """Pangenome shape: union index of 20 haplotypes, a prefilter trained on that index, 150 bp and
+    lognormal ~10 kbp reads with 95% random reads; answers equal the oracle's."""
+    rng = wl.rng_for(52)
+    k = 31
+    base = wl.random_bases(rng, 40_000, gc=0.41)
+    haps = wl.haplotypes(rng, base, 20)
+    built = sg.build_sbwt([h.tobytes() for h in haps], k)
+    lens = [150 if rng.random() < 0.9 else int(min(30_000, max(31, rng.lognormal(np.log(10_000), 0.5))))
+            for _ in range(600)]
+    rows = np.zeros(len(lens) + 1, dtype=np.uint64)
+    rows[1:] = np.cumsum(lens)
+    letters = wl.ACGT[rng.integers(0, 4, size=int(rows[-1]), dtype=np.uint8)]
+    for r in np.flatnonzero(rng.random(len(lens)) < 0.05).tolist():
+        h = haps[r % 20]
+        a, b = int(rows[r]), int(rows[r + 1])
+        s0 = int(rng.integers(0, h.size - (b - a) + 1)) if b - a <= h.size else 0
+        if b - a <= h.size:
+            letters[a:b] = wl.substitute(rng, h[s0:s0 + (b - a)].copy()[None, :], 0.01)[0]
+    with sg.Index.from_bits(built.bits, built.n_bits, k=k, k_presearch=12) as ix:
+        with sg.Prefilter.train(ix, steps=300, batch=2048, n_positive=300_000, n_negative=300_000, seed=3) as pf:
+            skipped, nk, want = _filtered_vs_oracle(ix, pf, built, letters, rows, k, 12, cuda)
+    assert 0 < skipped < nk

@@ -54,8 +54,11 @@ def test_pangenome_union_index(cuda):
     # queries: reads sampled from the haplotypes (positives) and random reads (negatives)
     reads = [wl.sampled_reads(rng, haps[i % 20], 20, 150, 0.0) for i in range(20)]
     pos = np.concatenate(reads)
+    # reads with 1% and 3% substitutions: found stretches broken by absent ones (backward steps, then
+    # fresh searches after each substitution)
+    subs = np.concatenate([wl.sampled_reads(rng, haps[i % 20], 10, 150, 0.01 if i % 2 else 0.03) for i in range(20)])
     neg = wl.uniform_reads(rng, 200, 150)
-    q = np.concatenate([pos, neg])
+    q = np.concatenate([pos, subs, neg])
     letters = np.ascontiguousarray(q).reshape(-1)
     rows = np.arange(q.shape[0] + 1, dtype=np.uint64) * np.uint64(150)
     ox = orc.OracleIndex(built.bits, built.n_bits)
@@ -65,3 +68,5 @@ def test_pangenome_union_index(cuda):
     assert np.array_equal(got, want)
     n_pos = pos.shape[0] * 120
     assert (got[:n_pos] != orc.NOT_FOUND).all()  # every haplotype k-mer is indexed
+    sub_hits = (got[n_pos:n_pos + subs.shape[0] * 120] != orc.NOT_FOUND).mean()
+    assert 0.2 < sub_hits < 0.95  # substituted reads mix found and absent k-mers
