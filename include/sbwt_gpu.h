@@ -242,8 +242,10 @@ int sbwt_search_reads_noalloc(sbwt_index *index, const uint8_t *d_letters, uint6
  * GPU in chunks with copies overlapped with compute.  While the index has
  * fewer than 2^32 columns and six or more OpenMP threads are available, the
  * answers cross PCIe as a membership bitmap plus the 32-bit node ids of the
- * found k-mers, and the host threads write the u64 answers; environment:
- * SBWT_PIPELINE_TRANSFER=dense|sparse forces one form,
+ * found k-mers, and the host threads write the u64 answers; with fewer
+ * threads a share of the chunks (sbwt_pipeline_dense_share) comes back as
+ * u64 answers by DMA into a pinned answer buffer instead; environment:
+ * SBWT_PIPELINE_TRANSFER=dense|sparse|hybrid forces one form,
  * SBWT_PIPELINE_CHUNK_LETTERS sets the chunk size (default 64M letters).
  * Replaces the
  * parse/position/search/copy-back chain of KmerSearch::search
@@ -251,6 +253,37 @@ int sbwt_search_reads_noalloc(sbwt_index *index, const uint8_t *d_letters, uint6
  * (results_persister.hpp:58-65). */
 int sbwt_search_reads_host(sbwt_index *index, const uint8_t *letters, uint64_t n_letters, const uint64_t *row_starts,
                            uint64_t n_rows, uint64_t *answers, uint64_t n_kmers);
+
+/* A batch in host memory searched on several index replicas, one per GPU
+ * (each loaded with its own sbwt_params.device; replicas may also share a
+ * device): the rows are cut into contiguous ranges of near-equal k-mer
+ * counts (sbwt_partition_rows; a row is never split), each replica runs
+ * sbwt_search_reads_host on its range from a host thread of its own and
+ * writes its disjoint slice of `answers`.  No data moves between the GPUs.
+ * The OpenMP threads of the call are shared among the replicas unless
+ * sbwt_set_host_threads set them.  The reference pins device 0
+ * (include/parameters.hpp:81). */
+int sbwt_search_reads_host_multi(sbwt_index *const *indexes, int n_indexes, const uint8_t *letters,
+                                 uint64_t n_letters, const uint64_t *row_starts, uint64_t n_rows, uint64_t *answers,
+                                 uint64_t n_kmers);
+/* bounds[0..n_parts]: row ranges [bounds[i], bounds[i+1]) of near-equal
+ * k-mer counts (each boundary the row boundary nearest to i/n_parts of the
+ * k-mers); needs no GPU. */
+int sbwt_partition_rows(const uint64_t *row_starts, uint64_t n_rows, uint32_t k, int n_parts, uint64_t *bounds);
+
+/* Host threads the host pipelines use (expansion of the sparse answers,
+ * row tables); 0 = the OpenMP default (OMP_NUM_THREADS).  No reference
+ * counterpart (its host side is one thread). */
+int sbwt_set_host_threads(sbwt_index *index, int threads);
+/* Share of the chunks of a sbwt_search_reads_host call whose u64 answers
+ * cross PCIe as such (the rest come back as bitmap + found node ids and are
+ * expanded by the host threads), for an index of n_columns searched with
+ * host_threads threads (0: the OpenMP default): 0 with six or more threads,
+ * D / (D + T E) below (D = 57 GB/s of copies, E = 11 GB/s of expansion per
+ * thread, T threads), 1 for indexes of 2^32 columns or more; the
+ * SBWT_PIPELINE_TRANSFER override included.  Needs no GPU.  No reference
+ * counterpart. */
+double sbwt_pipeline_dense_share(uint64_t n_columns, int host_threads);
 
 /* Bytes the last sbwt_search_reads_host or sbwt_search_reads_host_member
  * call on this index copied host->device (letters, row tables) and
@@ -290,16 +323,21 @@ uint64_t sbwt_count_kmers(const uint64_t *row_starts, uint64_t n_rows, uint32_t 
 
 /* Autotuner (no reference counterpart; the reference takes its kernel
  * variant from flags, include/parameters.hpp:79-297).  Times
- * sbwt_search_reads on the given device sample for every candidate launch
- * shape (line layout x k-mers per thread {1,2,3,4,6,8} x threads per k-mer
- * {1,2,4} x threads per block {128,256}; with SBWT_TUNE_POPPY also the poppy
- * layouts SB 512/1024/2048 with and without shuffles; with SBWT_TUNE_P also
- * presearch depths {8,10,12,14,15} <= k), checks that every candidate's answers
- * have the same checksum, and leaves the fastest configured on the index.
- * d_answers: device scratch of n_kmers u64.  report (optional): JSON of all
- * timings (fails if report_cap is too small). */
+ * sbwt_search_reads on the given device sample: (1) the search layout --
+ * 32-byte lines and the 512/2048-bit wide lines, with SBWT_TUNE_POPPY also
+ * the poppy layouts SB 512/1024/2048, with SBWT_TUNE_SHAPES also the
+ * per-k-mer kernel's shapes (k-mers per thread {1,2,3,4,6,8} x threads per
+ * k-mer {1,2,4} x threads per block {128,256}); (2) the run walk's knobs on
+ * the best layout (window 64/128/256 k-mers, resident blocks per SM, the
+ * evict-first policy of the table gathers, compact presearch entries); (3)
+ * with SBWT_TUNE_P the presearch depth {8,10,12,14,15} <= k.  Checks that
+ * every candidate's answers have the same checksum, and leaves the fastest
+ * configured on the index.  d_answers: device scratch of n_kmers u64.
+ * report (optional): JSON of the choice, the time of the configuration
+ * before tuning and every candidate (fails if report_cap is too small). */
 #define SBWT_TUNE_P 2u
 #define SBWT_TUNE_POPPY 4u
+#define SBWT_TUNE_SHAPES 8u
 int sbwt_autotune(sbwt_index *index, const uint8_t *d_letters, uint64_t n_letters, const uint64_t *d_row_starts,
                   uint64_t n_rows, uint64_t n_kmers, uint64_t *d_answers, uint32_t flags, char *report,
                   uint64_t report_cap);
@@ -386,8 +424,10 @@ int sbwt_mlp_logits(uint32_t k, const float *theta, const uint64_t *kmers, uint6
 /* Reads a FASTA query file the way KmerSearch::read_file does
  * (include/epicseq/kmer_search.hpp:319-342): every line that does not start
  * with '>' is one read; letters are concatenated.  Divergence: a last line
- * without '\n' keeps its last letter.  The returned buffers are owned by
- * the library (free with sbwt_queries_free). */
+ * without '\n' keeps its last letter.  A file whose first byte is '@' is read
+ * as FASTQ (four-line records; the sequence line is the read; no reference
+ * counterpart).  The returned buffers are owned by the library (free with
+ * sbwt_queries_free). */
 typedef struct {
     uint8_t *letters;     /* n_letters bytes (+32 zero bytes of padding) */
     uint64_t n_letters;
@@ -405,6 +445,18 @@ int sbwt_queries_read(const char *path, uint32_t k, sbwt_queries *out);
  * include/parameters.hpp:29). */
 int sbwt_queries_read_many(const char *const *paths, int n_files, uint32_t k, sbwt_queries *out, uint64_t *file_rows);
 void sbwt_queries_free(sbwt_queries *q);
+
+/* Streaming reader of one query file (FASTA as sbwt_queries_read, or FASTQ):
+ * sbwt_reader_next returns the next batch of whole reads, at most max_letters
+ * letters unless a single read is longer (0: the rest of the file); a batch
+ * with n_rows = 0 marks the end.  The file is read in 16 MiB blocks, so a
+ * caller can search one batch while the next is read.  Replaces the
+ * whole-file getline loop of KmerSearch::read_file (include/epicseq/
+ * kmer_search.hpp:319-342).  Batches are freed with sbwt_queries_free. */
+typedef struct sbwt_reader sbwt_reader;
+int sbwt_reader_open(const char *path, uint32_t k, sbwt_reader **out);
+int sbwt_reader_next(sbwt_reader *reader, uint64_t max_letters, sbwt_queries *out);
+void sbwt_reader_close(sbwt_reader *reader);
 
 /* Formats answers as the reference prints them (results_persister.hpp:82-95):
  * per read, each answer as a signed int64 followed by one space, then '\n'

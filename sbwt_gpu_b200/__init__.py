@@ -24,8 +24,8 @@ from ._lib import (CLI_PATH, LIB_PATH, SBWT_CUM_POPPY, SBWT_LAYOUT_LINES, SBWT_L
 
 __all__ = [
     "Index", "Params", "SbwtError", "build_sbwt", "write_index_files", "read_queries", "format_answers",
-    "count_kmers", "read_queries_many", "format_answers_device", "default_params", "SBWT_POPPY", "SBWT_CUM_POPPY", "SBWT_LAYOUT_LINES", "SBWT_LAYOUT_POPPY", "SBWT_LAYOUT_LINES512", "SBWT_LAYOUT_LINES2048",
-    "LIB_PATH", "CLI_PATH", "NOT_FOUND", "SEARCH_EVERY_KMER", "SEARCH_SKIP_ABSENT", "SEARCH_STREAM", "Prefilter", "mlp_params", "mlp_gradients", "mlp_logits", "MLP_PARAMS",
+    "count_kmers", "read_queries_many", "read_query_batches", "format_answers_device", "default_params", "SBWT_POPPY", "SBWT_CUM_POPPY", "SBWT_LAYOUT_LINES", "SBWT_LAYOUT_POPPY", "SBWT_LAYOUT_LINES512", "SBWT_LAYOUT_LINES2048",
+    "pipeline_dense_share", "partition_rows", "search_reads_host_multi", "LIB_PATH", "CLI_PATH", "NOT_FOUND", "SEARCH_EVERY_KMER", "SEARCH_SKIP_ABSENT", "SEARCH_STREAM", "Prefilter", "mlp_params", "mlp_gradients", "mlp_logits", "MLP_PARAMS",
 ]
 
 MLP_PARAMS = 256 * 128 + 256 + 256 * 256 + 256 + 256 + 1  # W1, b1, W2, b2, w3, b3
@@ -151,6 +151,10 @@ class Index:
         check(lib.sbwt_build_times(self._h, ms))
         return {"lines_ms": ms[0], "poppy_ms": ms[1], "presearch_ms": ms[2], "backward_ms": ms[3]}
 
+    def set_host_threads(self, threads):
+        """Host threads of the host pipelines (0: the OpenMP default)."""
+        check(lib.sbwt_set_host_threads(self._h, int(threads)))
+
     def pipeline_bytes(self):
         """Bytes the last host-buffer search (search_reads_host, member_reads_host) copied
         host->device and device->host."""
@@ -170,10 +174,12 @@ class Index:
         check(lib.sbwt_node_bytes_export(self._h, _ptr(out), n))
         return out
 
-    def autotune(self, d_letters, d_row_starts, d_answers, n_kmers, tune_p=False, tune_poppy=False):
-        """Times candidate launch shapes on a device sample, keeps the fastest; returns the JSON report."""
+    def autotune(self, d_letters, d_row_starts, d_answers, n_kmers, tune_p=False, tune_poppy=False,
+                 tune_shapes=False):
+        """Times candidate layouts and run-walk knobs (and p, poppy layouts, per-k-mer kernel shapes on
+        request) on a device sample, keeps the fastest; returns the JSON report."""
         n_rows = int(d_row_starts.numel()) - 1
-        flags = (2 if tune_p else 0) | (4 if tune_poppy else 0)
+        flags = (2 if tune_p else 0) | (4 if tune_poppy else 0) | (8 if tune_shapes else 0)
         buf = ctypes.create_string_buffer(1 << 16)
         check(lib.sbwt_autotune(self._h, _ptr(d_letters), int(d_letters.numel()), _ptr(d_row_starts), n_rows,
                                 int(n_kmers), _ptr(d_answers), flags, buf, len(buf)))
@@ -413,6 +419,29 @@ def read_queries(path, k):
     return letters, rows, nk
 
 
+def read_query_batches(path, k, max_letters):
+    """Streams a FASTA or FASTQ query file in batches of whole reads (sbwt_reader_next): yields
+    (letters uint8, row_starts uint64, n_kmers) per batch."""
+    h = c_void_p()
+    check(lib.sbwt_reader_open(os.fsencode(path), int(k), byref(h)))
+    try:
+        while True:
+            q = Queries()
+            check(lib.sbwt_reader_next(h, int(max_letters), byref(q)))
+            try:
+                if q.n_rows == 0:
+                    return
+                letters = np.ctypeslib.as_array(q.letters, shape=(q.n_letters + 32,))[: q.n_letters].copy() \
+                    if q.n_letters else np.zeros(0, dtype=np.uint8)
+                rows = np.ctypeslib.as_array(q.row_starts, shape=(q.n_rows + 1,)).copy()
+                nk = int(q.n_kmers)
+            finally:
+                lib.sbwt_queries_free(byref(q))
+            yield letters, rows, nk
+    finally:
+        lib.sbwt_reader_close(h)
+
+
 def read_queries_many(paths, k):
     """Several query files as one batch: (letters, row_starts, n_kmers, file_rows)."""
     arr = (ctypes.c_char_p * len(paths))(*[os.fsencode(p) for p in paths])
@@ -427,6 +456,35 @@ def read_queries_many(paths, k):
     finally:
         lib.sbwt_queries_free(byref(q))
     return letters, rows, nk, file_rows
+
+
+def pipeline_dense_share(n_columns, host_threads=0):
+    """Share of the chunks of a host-pipeline search whose u64 answers cross PCIe as such, for an index of
+    n_columns and host_threads threads (0: the OpenMP default); needs no GPU."""
+    return float(lib.sbwt_pipeline_dense_share(int(n_columns), int(host_threads)))
+
+
+def partition_rows(row_starts, k, n_parts):
+    """Row bounds (n_parts + 1) of contiguous ranges with near-equal k-mer counts (sbwt_partition_rows)."""
+    rs = np.ascontiguousarray(row_starts, dtype=np.uint64)
+    bounds = np.zeros(n_parts + 1, dtype=np.uint64)
+    check(lib.sbwt_partition_rows(_ptr(rs), rs.size - 1, int(k), int(n_parts), _ptr(bounds)))
+    return bounds
+
+
+def search_reads_host_multi(indexes, letters, row_starts, answers=None):
+    """Host reads searched on several index replicas (one per GPU), each on its own contiguous range of
+    rows; returns the host answers (sbwt_search_reads_host_multi)."""
+    letters = np.ascontiguousarray(letters, dtype=np.uint8)
+    rs = np.ascontiguousarray(row_starts, dtype=np.uint64)
+    k = indexes[0].info()["k"]
+    nk = int(lib.sbwt_count_kmers(_ptr(rs), rs.size - 1, k))
+    if answers is None:
+        answers = np.empty(max(nk, 1), dtype=np.uint64)
+    handles = (c_void_p * len(indexes))(*[ix._h.value if isinstance(ix._h, c_void_p) else ix._h for ix in indexes])
+    check(lib.sbwt_search_reads_host_multi(handles, len(indexes), _ptr(letters), letters.size, _ptr(rs), rs.size - 1,
+                                           _ptr(answers), nk))
+    return answers[:nk] if isinstance(answers, np.ndarray) else answers
 
 
 def count_kmers(row_starts, k):

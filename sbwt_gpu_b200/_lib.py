@@ -148,6 +148,11 @@ SIGNATURES = {
     "sbwt_search_kmers": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_void_p]),
     "sbwt_search_kmers_filtered": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_void_p, POINTER(c_uint64),
                                            c_void_p]),
+    "sbwt_search_reads_host_multi": (c_int, [c_void_p, c_int, c_void_p, c_uint64, c_void_p, c_uint64, c_void_p,
+                                             c_uint64]),
+    "sbwt_partition_rows": (c_int, [c_void_p, c_uint64, c_uint32, c_int, c_void_p]),
+    "sbwt_set_host_threads": (c_int, [c_void_p, c_int]),
+    "sbwt_pipeline_dense_share": (ctypes.c_double, [c_uint64, c_int]),
     "sbwt_search_reads_filtered": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_void_p,
                                            c_void_p, c_uint64, POINTER(c_uint64), c_void_p]),
     "sbwt_mlp_gradients": (c_int, [c_uint32, c_void_p, c_void_p, c_void_p, c_uint32, POINTER(ctypes.c_float),
@@ -158,6 +163,9 @@ SIGNATURES = {
     "sbwt_autotune": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_uint64, c_void_p, c_uint32, c_void_p,
                               c_uint64]),
     "sbwt_queries_free": (None, [POINTER(Queries)]),
+    "sbwt_reader_open": (c_int, [c_char_p, c_uint32, POINTER(c_void_p)]),
+    "sbwt_reader_next": (c_int, [c_void_p, c_uint64, POINTER(Queries)]),
+    "sbwt_reader_close": (None, [c_void_p]),
     "sbwt_format_answers": (c_int64, [c_void_p, c_uint64, c_uint32, c_void_p, c_void_p, c_uint64]),
     "sbwt_build": (c_int, [c_void_p, c_void_p, c_uint64, c_uint32, POINTER(Built)]),
     "sbwt_format_answers_device": (c_int, [c_void_p, c_uint64, c_uint32, c_void_p, c_uint64, c_void_p, c_uint64,

@@ -4,15 +4,24 @@
 // 81-209).
 //
 // On a caller-supplied sample batch (device letters + row starts) the tuner
-// times sbwt_search_reads for each candidate launch shape and keeps the
-// fastest: the queue-fed single-slot kernel and the line layout x k-mers per
-// thread {1,2,3,4,6,8} x threads per k-mer
-// {1,2,4} x threads per block {128,256}; optionally the reference's poppy
-// layouts (SB 512/1024/2048, with and without the cooperative "shuffles"
-// rank); and optionally presearch depths p in {8,10,12,14,15} (p <= k).  Every
-// candidate's answers are reduced to an order-sensitive checksum, and all
-// checksums must agree: the sweep doubles as a bit-exactness check across
-// shapes at full size.
+// times sbwt_search_reads for candidate configurations and keeps the
+// fastest, in stages:
+//   1. the search layout: 32-byte lines and the 512/2048-bit wide lines
+//      (the interleave granularity), with SBWT_TUNE_POPPY also the
+//      reference's poppy layouts (SB 512/1024/2048), with SBWT_TUNE_SHAPES
+//      also the per-k-mer kernel's register shapes (k-mers per thread
+//      {1,2,3,4,6,8} x threads per k-mer {1,2,4} x threads per block
+//      {128,256});
+//   2. the run walk's knobs on the best layout, one at a time, each kept
+//      when it is faster: window (64 / 256 k-mers against 128), resident
+//      blocks per SM, the evict-first policy of the presearch and
+//      backward-table gathers (never / always against by table size), and
+//      the compact 4-byte presearch entries;
+//   3. with SBWT_TUNE_P the presearch depth p in {8,10,12,14,15} (p <= k),
+//      then the window and the evict policy again at the chosen p.
+// Every candidate's answers are reduced to an order-sensitive checksum, and
+// all checksums must agree: the sweep doubles as a bit-exactness check
+// across configurations at full size.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -38,17 +47,25 @@ struct Cand {
     u32 kpt, tpk, tpb, sb;
     int shuffles;
     u32 p;
+    u32 window, bps;
+    int evict, compact;
     float ms;
     unsigned long long sum;
 };
 
+const char *layout_name(int l) {
+    return l == SBWT_LAYOUT_LINES ? "lines" : l == SBWT_LAYOUT_POPPY ? "poppy" : l == SBWT_LAYOUT_LINES512 ? "lines512"
+                                                                                                          : "lines2048";
+}
+
 std::string cand_json(const Cand &c) {
-    char b[256];
+    char b[384];
     std::snprintf(b, sizeof b,
                   "{\"layout\":\"%s\",\"kmers_per_thread\":%u,\"threads_per_kmer\":%u,\"threads_per_block\":%u,"
-                  "\"bits_in_superblock\":%u,\"shuffles\":%d,\"p\":%u,\"ms\":%.4f}",
-                  c.layout == SBWT_LAYOUT_LINES ? "lines" : "poppy", c.kpt, c.tpk, c.tpb, c.sb, c.shuffles, c.p,
-                  c.ms);
+                  "\"bits_in_superblock\":%u,\"shuffles\":%d,\"p\":%u,\"window\":%u,\"blocks_per_sm\":%u,"
+                  "\"evict\":\"%s\",\"compact_presearch\":%d,\"ms\":%.4f}",
+                  layout_name(c.layout), c.kpt, c.tpk, c.tpb, c.sb, c.shuffles, c.p, c.window, c.bps,
+                  c.evict == 0 ? "by table size" : c.evict == 1 ? "never" : "always", c.compact, c.ms);
     return b;
 }
 
@@ -71,10 +88,12 @@ extern "C" int sbwt_autotune(sbwt_index *ix, const uint8_t *d_letters, uint64_t 
     int rc = 0;
     const KernelShape saved = ix->shape;
     const u32 saved_p = ix->p;
+    const int saved_compact = ix->compact_pre;
     const bool saved_graph = ix->use_graph, saved_prof = ix->prof_on;
     ix->use_graph = false;
     ix->prof_on = false;
     std::vector<Cand> done;
+    float default_ms = 0.0f;
     unsigned long long want_sum = 0;
     bool have_sum = false;
 
@@ -82,6 +101,7 @@ extern "C" int sbwt_autotune(sbwt_index *ix, const uint8_t *d_letters, uint64_t 
         if (c.layout == SBWT_LAYOUT_POPPY) {
             if (!ix->poppy_ok || ix->sb != c.sb || ix->kind != SBWT_POPPY) SBWT_TRY(build_poppy(ix, c.sb, SBWT_POPPY, s));
         }
+        if (wide_sectors(c.layout) && ix->wide_s != wide_sectors(c.layout)) SBWT_TRY(build_wide(ix, wide_sectors(c.layout), s));
         ix->shape.layout = c.layout;
         ix->shape.kpt = c.kpt;
         ix->shape.tpk = c.tpk;
@@ -89,7 +109,14 @@ extern "C" int sbwt_autotune(sbwt_index *ix, const uint8_t *d_letters, uint64_t 
         ix->shape.sb = c.sb;
         ix->shape.kind = SBWT_POPPY;
         ix->shape.shuffles = c.shuffles;
-        if (c.p != ix->p) SBWT_TRY(run_presearch(ix, c.p, s));
+        ix->shape.window = c.window;
+        ix->shape.blocks_per_sm = c.bps;
+        ix->shape.evict = c.evict;
+        if (c.p != ix->p || c.compact != ix->compact_pre) {
+            ix->compact_pre = c.compact;
+            SBWT_TRY(run_presearch(ix, c.p, s));
+        }
+        ix->gen++;
         return 0;
     };
     auto measure = [&](Cand &c) -> int {
@@ -130,12 +157,20 @@ extern "C" int sbwt_autotune(sbwt_index *ix, const uint8_t *d_letters, uint64_t 
             break;
         }
         const u32 p0 = saved_p;
+        const int c0 = ix->compact_pre;
+        // stage 1: layouts; the first candidate is the index's configuration before tuning
         std::vector<Cand> stage1;
+        stage1.push_back(Cand{saved.layout, saved.kpt, saved.tpk, saved.tpb, saved.sb, saved.shuffles, p0,
+                              saved.window, saved.blocks_per_sm, saved.evict, c0, 0, 0});
         if (ix->lines_ok) {
-            stage1.push_back(Cand{SBWT_LAYOUT_LINES, 0, 1, 128, 1024, 0, p0, 0, 0});  // queue-fed single slot
-            for (u32 tpb : {128u, 256u})
-                for (u32 tpk : {1u, 2u, 4u})
-                    for (u32 kpt : {1u, 2u, 3u, 4u, 6u, 8u}) stage1.push_back(Cand{SBWT_LAYOUT_LINES, kpt, tpk, tpb, 1024, 0, p0, 0, 0});
+            for (int l : {SBWT_LAYOUT_LINES, SBWT_LAYOUT_LINES512, SBWT_LAYOUT_LINES2048})
+                if (!(l == saved.layout && saved.kpt == 0 && saved.tpk == 1))
+                    stage1.push_back(Cand{l, 0, 1, 128, 1024, 0, p0, 128, 0, 0, c0, 0, 0});
+            if (flags & 8u)
+                for (u32 tpb : {128u, 256u})
+                    for (u32 tpk : {1u, 2u, 4u})
+                        for (u32 kpt : {1u, 2u, 3u, 4u, 6u, 8u})
+                            stage1.push_back(Cand{SBWT_LAYOUT_LINES, kpt, tpk, tpb, 1024, 0, p0, 128, 0, 0, c0, 0, 0});
         }
         if ((flags & 4u) || !ix->lines_ok)
             for (u32 sb : {512u, 1024u, 2048u})
@@ -143,38 +178,68 @@ extern "C" int sbwt_autotune(sbwt_index *ix, const uint8_t *d_letters, uint64_t 
                     if (sh && sb == 512) continue;
                     for (u32 kpt : {0u, 1u, 2u}) {
                         if (kpt == 0 && sh) continue;
-                        stage1.push_back(Cand{SBWT_LAYOUT_POPPY, kpt, 1, kpt == 0 ? 128u : 256u, sb, sh, p0, 0, 0});
+                        if (kpt && !(flags & 8u)) continue;
+                        stage1.push_back(Cand{SBWT_LAYOUT_POPPY, kpt, 1, kpt == 0 ? 128u : 256u, sb, sh, p0, 128, 0, 0,
+                                              c0, 0, 0});
                     }
                 }
         for (Cand &c : stage1)
             if ((rc = measure(c)) != 0) break;
         if (rc) break;
-        std::vector<Cand> ranked = done;
-        std::sort(ranked.begin(), ranked.end(), [](const Cand &a, const Cand &b) { return a.ms < b.ms; });
-        Cand best = ranked.front();
-        if (flags & 2u) {
-            for (u32 p : {8u, 10u, 12u, 14u, 15u}) {
-                if (p > ix->k || p == best.p) continue;
+        default_ms = done.front().ms;
+        Cand best = *std::min_element(done.begin(), done.end(), [](const Cand &a, const Cand &b) { return a.ms < b.ms; });
+        // stage 2: the run walk's knobs, one at a time (kept when faster by more than 1 %)
+        auto try_knob = [&](Cand c) -> int {
+            SBWT_TRY(measure(c));
+            if (c.ms < 0.99f * best.ms) best = c;
+            return 0;
+        };
+        auto walk_knobs = [&](bool grid, bool compact) -> int {
+            if (best.kpt != 0) return 0;  // the per-k-mer kernel has none of these knobs
+            if (best.layout == SBWT_LAYOUT_LINES)
+                for (u32 w : {64u, 256u}) {
+                    Cand c = best;
+                    c.window = w;
+                    SBWT_TRY(try_knob(c));
+                }
+            for (int ev : {1, 2}) {
                 Cand c = best;
+                c.evict = ev;
+                SBWT_TRY(try_knob(c));
+            }
+            if (grid)
+                for (u32 b : {4u, 6u, 7u, 8u}) {
+                    Cand c = best;
+                    c.bps = b;
+                    SBWT_TRY(try_knob(c));
+                }
+            if (compact && ix->n < dev::kPreMaxColumns && best.p) {
+                Cand c = best;
+                c.compact = best.compact == 1 ? 0 : 1;
+                SBWT_TRY(try_knob(c));
+            }
+            return 0;
+        };
+        if ((rc = walk_knobs(true, true)) != 0) break;
+        // stage 3: presearch depth, then the knobs that depend on the tables' sizes again
+        if (flags & 2u) {
+            const Cand before = best;
+            for (u32 p : {8u, 10u, 12u, 14u, 15u}) {
+                if (p > ix->k || p == before.p) continue;
+                Cand c = before;
                 c.p = p;
-                if ((rc = measure(c)) != 0) break;
-                if (c.ms < best.ms) best = c;
+                if ((rc = try_knob(c)) != 0) break;
             }
             if (rc) break;
-            // re-rank the five best shapes at the chosen p
-            for (size_t i = 0; i < ranked.size() && i < 5; i++) {
-                Cand c = ranked[i];
-                if (c.p == best.p) continue;
-                c.p = best.p;
-                if ((rc = measure(c)) != 0) break;
-                if (c.ms < best.ms) best = c;
-            }
-            if (rc) break;
+            if (best.p != before.p && (rc = walk_knobs(false, true)) != 0) break;
         }
         if ((rc = apply(best)) != 0) break;
         if (report && report_cap) {
-            std::string j = "{\"best\":" + cand_json(best) + ",\"n_kmers\":" + std::to_string(n_kmers) +
-                            ",\"checksum\":" + std::to_string(want_sum) + ",\"candidates\":[";
+            char dm[32];
+            std::snprintf(dm, sizeof dm, "%.4f", default_ms);
+            std::string j = "{\"best\":" + cand_json(best) + ",\"default_ms\":" + dm +
+                            ",\"n_kmers\":" + std::to_string(n_kmers) + ",\"checksum\":" + std::to_string(want_sum) +
+                            ",\"candidates\":[";
             for (size_t i = 0; i < done.size(); i++) j += (i ? "," : "") + cand_json(done[i]);
             j += "]}";
             if (j.size() + 1 > report_cap) {
@@ -186,7 +251,10 @@ extern "C" int sbwt_autotune(sbwt_index *ix, const uint8_t *d_letters, uint64_t 
     } while (false);
     if (rc) {  // restore the previous configuration
         ix->shape = saved;
-        if (ix->p != saved_p) run_presearch(ix, saved_p, s);
+        if (ix->p != saved_p || ix->compact_pre != saved_compact) {
+            ix->compact_pre = saved_compact;
+            run_presearch(ix, saved_p, s);
+        }
     }
     ix->use_graph = saved_graph;
     ix->prof_on = saved_prof;

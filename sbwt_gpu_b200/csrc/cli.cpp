@@ -13,6 +13,12 @@
 //               [--kmers-per-thread=N] [--threads-per-kmer=1|2|4]
 //               [--search-mode=every|skip|stream]
 //
+// The query file (FASTA, or FASTQ when its first byte is '@') is read by a
+// thread of its own in batches of whole reads (sbwt_reader_next) while the
+// previous batch is searched, formatted and written, so file reading
+// overlaps the search instead of preceding it (the reference reads the whole
+// file first, include/epicseq/kmer_search.hpp:319-342).
+//
 // Differences from the reference: errors return a non-zero exit status
 // (the reference always returns 0, src/search.cpp:14-25); --rank-structure=
 // flat-poppy, which the reference parses but never implements
@@ -20,11 +26,15 @@
 // --rank-word-size (unused on the reference's live path) are accepted and
 // ignored.
 #include <chrono>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
+#include <mutex>
 #include <regex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -132,17 +142,20 @@ int parse(int argc, char **argv, Options &o) {
 }
 
 // Searches the reads of q in batches of at most kBatchLetters letters and
-// writes the reference's text for them to `out`.
-constexpr uint64_t kBatchLetters = 1ull << 28;
+// writes the reference's text for them to `out`.  The device buffers persist
+// across calls.  The environment variable SBWT_CLI_BATCH_LETTERS sets
+// another batch size (also the size of the reader's batches).
+uint64_t kBatchLetters = 1ull << 28;
 
-int search_and_write(sbwt_index *ix, const sbwt_queries &q, uint32_t k, FILE *out) {
+struct Writer {
     uint8_t *d_letters = nullptr;
     uint64_t *d_rows = nullptr, *d_ans = nullptr;
     char *d_text = nullptr, *h_text = nullptr;
-    uint64_t cap_l = 0, cap_r = 0, cap_a = 0, cap_t = 0;
+    uint64_t cap_l = 0, cap_r = 0, cap_a = 0, cap_t = 0, cap_h = 0;
     std::vector<uint64_t> rows;
-    int rc = 0;
-    auto grow = [](auto *&p, uint64_t &cap, uint64_t need) {
+
+    template <class T>
+    static bool grow(T *&p, uint64_t &cap, uint64_t need) {
         if (need <= cap) return true;
         cudaFree(p);
         p = nullptr;
@@ -150,63 +163,119 @@ int search_and_write(sbwt_index *ix, const sbwt_queries &q, uint32_t k, FILE *ou
         if (cudaMalloc((void **)&p, need * sizeof(*p)) != cudaSuccess) return false;
         cap = need;
         return true;
-    };
-    uint64_t r0 = 0;
-    while (rc == 0 && r0 < q.n_rows) {
-        // rows [r0, r1): at least one, at most kBatchLetters letters unless one read is longer
-        uint64_t r1 = r0 + 1;
-        while (r1 < q.n_rows && q.row_starts[r1 + 1] - q.row_starts[r0] <= kBatchLetters) r1++;
-        const uint64_t base = q.row_starts[r0], nl = q.row_starts[r1] - base, nr = r1 - r0;
-        rows.resize(nr + 1);
-        uint64_t nk = 0;
-        for (uint64_t r = 0; r <= nr; r++) {
-            rows[r] = q.row_starts[r0 + r] - base;
-            if (r < nr) {
-                const uint64_t len = q.row_starts[r0 + r + 1] - q.row_starts[r0 + r];
-                nk += len >= k ? len - k + 1 : 0;
-            }
-        }
-        uint64_t bytes = 0;
-        if (!grow(d_letters, cap_l, nl + 1) || !grow(d_rows, cap_r, nr + 1) || !grow(d_ans, cap_a, nk + 1)) {
-            rc = 1;
-            break;
-        }
-        if (cudaMemcpy(d_letters, q.letters + base, nl, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(d_rows, rows.data(), (nr + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice) != cudaSuccess) {
-            rc = 1;
-            break;
-        }
-        if (nk && sbwt_search_reads(ix, d_letters, nl, d_rows, nr, d_ans, nullptr, nk, nullptr)) {
-            rc = 1;
-            break;
-        }
-        if (sbwt_format_answers_device(d_rows, nr, k, d_ans, nk, nullptr, 0, &bytes, nullptr) ||
-            !grow(d_text, cap_t, bytes + 1)) {
-            rc = 1;
-            break;
-        }
-        if (sbwt_format_answers_device(d_rows, nr, k, d_ans, nk, d_text, cap_t, &bytes, nullptr)) {
-            rc = 1;
-            break;
-        }
-        cudaFreeHost(h_text);
-        h_text = nullptr;
-        if (cudaMallocHost((void **)&h_text, bytes + 1) != cudaSuccess ||
-            cudaMemcpy(h_text, d_text, bytes, cudaMemcpyDeviceToHost) != cudaSuccess ||
-            std::fwrite(h_text, 1, bytes, out) != bytes) {
-            rc = 1;
-            break;
-        }
-        r0 = r1;
     }
-    std::fflush(out);
-    cudaFree(d_letters);
-    cudaFree(d_rows);
-    cudaFree(d_ans);
-    cudaFree(d_text);
-    cudaFreeHost(h_text);
-    return rc;
-}
+
+    ~Writer() {
+        cudaFree(d_letters);
+        cudaFree(d_rows);
+        cudaFree(d_ans);
+        cudaFree(d_text);
+        cudaFreeHost(h_text);
+    }
+
+    int run(sbwt_index *ix, const sbwt_queries &q, uint32_t k, FILE *out) {
+        uint64_t r0 = 0;
+        while (r0 < q.n_rows) {
+            // rows [r0, r1): at least one, at most kBatchLetters letters unless one read is longer
+            uint64_t r1 = r0 + 1;
+            while (r1 < q.n_rows && q.row_starts[r1 + 1] - q.row_starts[r0] <= kBatchLetters) r1++;
+            const uint64_t base = q.row_starts[r0], nl = q.row_starts[r1] - base, nr = r1 - r0;
+            rows.resize(nr + 1);
+            uint64_t nk = 0;
+            for (uint64_t r = 0; r <= nr; r++) {
+                rows[r] = q.row_starts[r0 + r] - base;
+                if (r < nr) {
+                    const uint64_t len = q.row_starts[r0 + r + 1] - q.row_starts[r0 + r];
+                    nk += len >= k ? len - k + 1 : 0;
+                }
+            }
+            uint64_t bytes = 0;
+            if (!grow(d_letters, cap_l, nl + 1) || !grow(d_rows, cap_r, nr + 1) || !grow(d_ans, cap_a, nk + 1))
+                return 1;
+            if (cudaMemcpy(d_letters, q.letters + base, nl, cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemcpy(d_rows, rows.data(), (nr + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice) != cudaSuccess)
+                return 1;
+            if (nk && sbwt_search_reads(ix, d_letters, nl, d_rows, nr, d_ans, nullptr, nk, nullptr)) return 1;
+            if (sbwt_format_answers_device(d_rows, nr, k, d_ans, nk, nullptr, 0, &bytes, nullptr) ||
+                !grow(d_text, cap_t, bytes + 1))
+                return 1;
+            if (sbwt_format_answers_device(d_rows, nr, k, d_ans, nk, d_text, cap_t, &bytes, nullptr)) return 1;
+            if (bytes + 1 > cap_h) {
+                cudaFreeHost(h_text);
+                h_text = nullptr;
+                cap_h = 0;
+                if (cudaMallocHost((void **)&h_text, bytes + 1) != cudaSuccess) return 1;
+                cap_h = bytes + 1;
+            }
+            if (cudaMemcpy(h_text, d_text, bytes, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                std::fwrite(h_text, 1, bytes, out) != bytes)
+                return 1;
+            r0 = r1;
+        }
+        return 0;
+    }
+};
+
+// Reads the query file's batches on a thread of its own, at most two ahead
+// of the consumer.
+struct Prefetch {
+    sbwt_reader *rd = nullptr;
+    uint32_t k = 31;
+    std::mutex m;
+    std::condition_variable cv;
+    std::deque<sbwt_queries> ready;
+    bool done = false;
+    std::string error;
+    double read_ms = 0;  // time the reader thread spent reading
+    std::thread th;
+
+    void start() {
+        th = std::thread([this] {
+            for (;;) {
+                {
+                    std::unique_lock<std::mutex> lk(m);
+                    cv.wait(lk, [this] { return ready.size() < 2 || done; });
+                    if (done) return;
+                }
+                const auto t = std::chrono::steady_clock::now();
+                sbwt_queries q;
+                const int rc = sbwt_reader_next(rd, kBatchLetters, &q);
+                const double ms = ms_since(t);
+                std::lock_guard<std::mutex> lk(m);
+                read_ms += ms;
+                if (rc) error = sbwt_last_error();
+                if (rc || q.n_rows == 0) {
+                    if (!rc) sbwt_queries_free(&q);
+                    done = true;
+                    cv.notify_all();
+                    return;
+                }
+                ready.push_back(q);
+                cv.notify_all();
+            }
+        });
+    }
+    // The next batch, or false at the end (or on an error: see `error`).
+    bool next(sbwt_queries &q) {
+        std::unique_lock<std::mutex> lk(m);
+        cv.wait(lk, [this] { return !ready.empty() || done; });
+        if (ready.empty()) return false;
+        q = ready.front();
+        ready.pop_front();
+        cv.notify_all();
+        return true;
+    }
+    void stop() {
+        {
+            std::lock_guard<std::mutex> lk(m);
+            done = true;
+            cv.notify_all();
+        }
+        if (th.joinable()) th.join();
+        for (auto &q : ready) sbwt_queries_free(&q);
+        ready.clear();
+    }
+};
 
 }  // namespace
 
@@ -239,40 +308,67 @@ int main(int argc, char **argv) {
         return 1;
     }
     cudaDeviceSetLimit(cudaLimitMaxL2FetchGranularity, o.limit_search);  // search_caller.hpp:91-96
+    if (const char *e = std::getenv("SBWT_CLI_BATCH_LETTERS")) {
+        const unsigned long long v = std::strtoull(e, nullptr, 10);
+        if (v) kBatchLetters = v;
+    }
     auto t1 = std::chrono::steady_clock::now();
-    sbwt_queries q;
-    if (sbwt_queries_read(o.queries.c_str(), o.p.k, &q)) {
+    Prefetch pf;
+    pf.k = o.p.k;
+    if (sbwt_reader_open(o.queries.c_str(), o.p.k, &pf.rd)) {
         std::fprintf(stderr, "%s\n", sbwt_last_error());
         sbwt_index_free(ix);
         return 1;
     }
-    const double ms_read = ms_since(t1);
+    pf.start();
     int rc = 0;
-    auto t2 = std::chrono::steady_clock::now();
-    if (o.store) {
-        // batches of whole reads: letters + offsets to the device, search, text formatted on the
-        // device (sbwt_format_answers_device), text back and written in read order
-        if (search_and_write(ix, q, o.p.k, stdout)) {
-            const char *msg = sbwt_last_error();
-            std::fprintf(stderr, "%s\n", msg && *msg ? msg : cudaGetErrorString(cudaGetLastError()));
-            rc = 1;
+    uint64_t n_kmers = 0;
+    double wait_ms = 0;
+    {
+        Writer wr;
+        std::vector<uint64_t> answers;
+        for (;;) {
+            const auto tw = std::chrono::steady_clock::now();
+            sbwt_queries q;
+            const bool more = pf.next(q);
+            wait_ms += ms_since(tw);
+            if (!more) break;
+            n_kmers += q.n_kmers;
+            if (o.store) {
+                // letters + offsets to the device, search, text formatted on the device
+                // (sbwt_format_answers_device), text back and written in read order
+                if (wr.run(ix, q, o.p.k, stdout)) {
+                    const char *msg = sbwt_last_error();
+                    std::fprintf(stderr, "%s\n", msg && *msg ? msg : cudaGetErrorString(cudaGetLastError()));
+                    rc = 1;
+                }
+            } else {
+                answers.resize(q.n_kmers ? q.n_kmers : 1);
+                if (sbwt_search_reads_host(ix, q.letters, q.n_letters, q.row_starts, q.n_rows, answers.data(),
+                                           q.n_kmers)) {
+                    std::fprintf(stderr, "%s\n", sbwt_last_error());
+                    rc = 1;
+                }
+            }
+            sbwt_queries_free(&q);
+            if (rc) break;
         }
-    } else {
-        std::vector<uint64_t> answers(q.n_kmers ? q.n_kmers : 1);
-        if (sbwt_search_reads_host(ix, q.letters, q.n_letters, q.row_starts, q.n_rows, answers.data(), q.n_kmers)) {
-            std::fprintf(stderr, "%s\n", sbwt_last_error());
-            rc = 1;
-        }
+        std::fflush(stdout);
     }
-    const double ms_search = ms_since(t2);
-    std::fprintf(stderr, "Reading the query file: %f ms.\n", ms_read);
+    pf.stop();
+    sbwt_reader_close(pf.rd);
+    if (!rc && !pf.error.empty()) {
+        std::fprintf(stderr, "%s\n", pf.error.c_str());
+        rc = 1;
+    }
+    const double ms_total = ms_since(t1);
+    std::fprintf(stderr, "Reading the query file: %f ms (on its own thread, overlapped with the search; %f ms "
+                         "waiting for it).\n", pf.read_ms, wait_ms);
     std::fprintf(stderr, "Search (host to device, pack, search%s, device to host): %f ms.\n",
-                 o.store ? ", answer text, writing" : "", ms_search);
-    std::fprintf(stderr, "Number of k-mers queried: %llu\n", (unsigned long long)q.n_kmers);
-    if (q.n_kmers)
-        std::fprintf(stderr, "Total per query: %f ns.\n", ms_search * 1e6 / (double)q.n_kmers);
+                 o.store ? ", answer text, writing" : "", ms_total - wait_ms);
+    std::fprintf(stderr, "Number of k-mers queried: %llu\n", (unsigned long long)n_kmers);
+    if (n_kmers) std::fprintf(stderr, "Total per query: %f ns.\n", ms_total * 1e6 / (double)n_kmers);
     if (!o.store) std::fprintf(stderr, "The results are not stored to the file.\n");
-    sbwt_queries_free(&q);
     sbwt_index_free(ix);
     std::fprintf(stderr, "%f ms in total, from the start of main.\n", ms_since(t_main));
     return rc;

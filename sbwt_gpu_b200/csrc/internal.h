@@ -159,6 +159,8 @@ struct sbwt_index {
     cudaStream_t pipe_stream[kPipeSlots] = {nullptr, nullptr, nullptr, nullptr};
     // bytes the last host-pipeline call copied host->device and device->host
     uint64_t pipe_h2d = 0, pipe_d2h = 0;
+    // host threads of the host pipelines (0: the OpenMP default)
+    int host_threads = 0;
     // bumped whenever a device structure a search reads is rebuilt (graph keys)
     uint64_t gen = 1;
     bool use_graph = false;

@@ -22,6 +22,8 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <string>
+#include <thread>
 #include <vector>
 #if defined(__x86_64__)
 #include <emmintrin.h>
@@ -80,23 +82,44 @@ constexpr u32 kGroupWords = 64;
 constexpr u32 kGroupWarps = 4;  // groups (warps) per block of group_nodes_kernel
 
 // How a chunk's answers cross PCIe: u64 answers (dense), the sparse form, or
-// both (hybrid: every kHybridPeriod-th chunk dense, copied straight into the
-// caller's pinned buffer by the copy engines while the host threads expand
-// the sparse ones).  Sparse needs 32-bit node ids and enough host threads
-// to expand faster than PCIe brings u64 answers (about 11 GB/s of answers
-// per thread against 57 GB/s).  The environment variable
-// SBWT_PIPELINE_TRANSFER = dense | sparse | hybrid overrides the choice.
-enum Transfer { kDense, kSparse, kHybrid };
+// both (split: some chunks dense, copied straight into the caller's pinned
+// buffer by the copy engines while the host threads expand the sparse
+// ones).  Sparse needs 32-bit node ids.  With T host threads the expansion
+// writes about kExpandPerThread bytes of answers per second per thread, the
+// copy engines kDmaBytes: with many threads (T >= kMinExpandThreads) every
+// chunk is sparse (the copy engines' writes into host memory would only
+// contend with the expansion's, measured slower); with fewer, the share of
+// dense chunks that lets both finish together, f = D / (D + T x E), spread
+// evenly over the chunks (2 threads, as under torchrun with 8 ranks on 16
+// cores: 72 % dense, about 1.4x the all-dense time; 1 thread: 84 %).  The
+// environment variable SBWT_PIPELINE_TRANSFER = dense | sparse | hybrid
+// (every fourth chunk dense) overrides the choice.
+enum Transfer { kDense, kSparse, kSplit };
 constexpr int kMinExpandThreads = 6;
-constexpr u64 kHybridPeriod = 4;
+constexpr double kExpandPerThread = 11e9;  // bytes of u64 answers per second per host thread (measured)
+constexpr double kDmaBytes = 57e9;         // device->host copy, bytes per second (measured)
 
-Transfer transfer_mode(const sbwt_index *ix) {
-    if (ix->n > 0xffffffffull) return kDense;
+int host_threads(const sbwt_index *ix) { return ix->host_threads > 0 ? ix->host_threads : omp_get_max_threads(); }
+
+// Share of chunks whose u64 answers cross PCIe as such (the rest sparse),
+// for an index of n columns searched with T host threads.
+double dense_share(u64 n, int T, Transfer *mode) {
+    Transfer t;
+    double f;
     const char *e = std::getenv("SBWT_PIPELINE_TRANSFER");
-    if (e && std::strcmp(e, "dense") == 0) return kDense;
-    if (e && std::strcmp(e, "sparse") == 0) return kSparse;
-    if (e && std::strcmp(e, "hybrid") == 0) return kHybrid;
-    return omp_get_max_threads() >= kMinExpandThreads ? kSparse : kDense;
+    if (n > 0xffffffffull || (e && std::strcmp(e, "dense") == 0)) {
+        t = kDense, f = 1.0;
+    } else if (e && std::strcmp(e, "sparse") == 0) {
+        t = kSparse, f = 0.0;
+    } else if (e && std::strcmp(e, "hybrid") == 0) {
+        t = kSplit, f = 0.25;
+    } else if (T >= kMinExpandThreads) {
+        t = kSparse, f = 0.0;
+    } else {
+        t = kSplit, f = kDmaBytes / (kDmaBytes + T * kExpandPerThread);
+    }
+    if (mode) *mode = t;
+    return f;
 }
 
 // gcnt[g] = found k-mers of group g; gcnt[ng] = 0 (the exclusive scan's total).
@@ -152,9 +175,9 @@ __global__ void __launch_bounds__(32 * kGroupWarps) group_nodes_kernel(const uin
 // stores: the answers are not read back by this thread).  nodes may be read
 // one element past the chunk's found ids (a select instead of a branch), so
 // its buffer has slack.
-void expand_answers(u64 *answers, u64 nk, const uint32_t *member, const u64 *goff, const uint32_t *nodes) {
+void expand_answers(u64 *answers, u64 nk, const uint32_t *member, const u64 *goff, const uint32_t *nodes, int threads) {
     const u64 nw = (nk + 31) / 32, ng = (nw + kGroupWords - 1) / kGroupWords;
-#pragma omp parallel if (nk > (1u << 16))
+#pragma omp parallel num_threads(threads) if (nk > (1u << 16))
     {
 #pragma omp for schedule(static)
         for (int64_t g = 0; g < (int64_t)ng; g++) {
@@ -239,12 +262,17 @@ int pipeline_chunks(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, 
     for (int i = 0; i < kSlots; i++)
         if (!ix->pipe_stream[i]) SBWT_CHECK_CUDA(cudaStreamCreateWithFlags(&ix->pipe_stream[i], cudaStreamNonBlocking));
     const bool pin_in = is_pinned(letters);
-    const Transfer xfer = answers ? transfer_mode(ix) : kDense;
-    const bool sparse = xfer != kDense;  // some chunks come back in sparse form
+    const int threads = host_threads(ix);
     const bool pin_out = answers && (n_kmers == 0 || is_pinned(answers));
-    // dense chunks: all of them, or (hybrid, into a pinned buffer) every kHybridPeriod-th
+    Transfer xfer = kDense;
+    double share = answers ? dense_share(ix->n, threads, &xfer) : 1.0;
+    if (xfer == kSplit && !pin_out) xfer = kSparse, share = 0.0;  // dense chunks go straight into a pinned buffer
+    const bool sparse = answers && xfer != kDense;  // some chunks come back in sparse form
+    // dense chunks: all of them, or (split) chunk b when floor((b+1) f) > floor(b f), f spread evenly
     auto dense_chunk = [&](size_t b) {
-        return xfer == kDense || (xfer == kHybrid && pin_out && b % kHybridPeriod == kHybridPeriod - 1);
+        if (xfer == kDense) return true;
+        if (xfer == kSparse) return false;
+        return (u64)((double)(b + 1) * share) > (u64)((double)b * share);
     };
     ix->pipe_h2d = ix->pipe_d2h = 0;
     u64 max_letters = 0, max_rows = 0, max_k = 0;
@@ -315,7 +343,7 @@ int pipeline_chunks(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, 
             const Chunk &c = chunks[(size_t)pending[slot]];
             Workspace &w = ix->ws[slot];
             if (sparse) {
-                expand_answers(answers + c.k0, c.nk, w.h_member, w.h_goff, w.h_nodes);
+                expand_answers(answers + c.k0, c.nk, w.h_member, w.h_goff, w.h_nodes, threads);
             } else if (answers) {
                 std::memcpy(answers + c.k0, w.h_answers, c.nk * sizeof(u64));
             } else {
@@ -439,4 +467,104 @@ extern "C" int sbwt_search_reads_host_member(sbwt_index *ix, const uint8_t *lett
     clear_error();
     if (n_kmers && !member_bits) return set_error("NULL host pointer");
     return run_pipeline(ix, letters, n_letters, row_starts, n_rows, nullptr, member_bits, n_kmers);
+}
+
+extern "C" int sbwt_set_host_threads(sbwt_index *ix, int threads) {
+    clear_error();
+    if (!ix) return set_error("index is NULL");
+    if (threads < 0) return set_error("host threads must be >= 0 (0: the OpenMP default)");
+    ix->host_threads = threads;
+    return 0;
+}
+
+extern "C" double sbwt_pipeline_dense_share(uint64_t n_columns, int host_threads) {
+    return dense_share(n_columns, host_threads > 0 ? host_threads : omp_get_max_threads(), nullptr);
+}
+
+// ------------------------------------------------------------ several GPUs
+//
+// A batch in host memory spread over several index replicas (one per GPU):
+// the rows are cut into contiguous ranges of near-equal k-mer counts (a row
+// is never split), each replica runs the host pipeline on its range from a
+// host thread of its own, and writes its disjoint slice of the caller's
+// answers.  No exchange between the GPUs: the index is read-only and every
+// k-mer independent.  The reference pins device 0 (include/parameters.hpp:81).
+
+extern "C" int sbwt_partition_rows(const uint64_t *row_starts, uint64_t n_rows, uint32_t k, int n_parts,
+                                   uint64_t *bounds) {
+    clear_error();
+    if (!row_starts || !bounds || n_parts < 1) return set_error("sbwt_partition_rows: bad arguments");
+    // k-mers before each row, then the first row at or past each part's share
+    std::vector<u64> before(n_rows + 1);
+    u64 t = 0;
+    for (u64 r = 0; r < n_rows; r++) {
+        before[r] = t;
+        if (row_starts[r + 1] < row_starts[r]) return set_error("row_starts must be non-decreasing (row %llu)",
+                                                                (unsigned long long)r);
+        const u64 len = row_starts[r + 1] - row_starts[r];
+        t += len >= k ? len - k + 1 : 0;
+    }
+    before[n_rows] = t;
+    bounds[0] = 0;
+    for (int i = 1; i < n_parts; i++) {
+        const u64 target = (u64)((unsigned __int128)t * (unsigned)i / (unsigned)n_parts);
+        // the row boundary whose k-mer count before it is nearest to the target
+        u64 r = (u64)(std::lower_bound(before.begin(), before.end(), target) - before.begin());
+        if (r > 0 && target - before[r - 1] < before[r] - target) r--;
+        bounds[i] = std::max<u64>(r, bounds[i - 1]);
+    }
+    bounds[n_parts] = n_rows;
+    return 0;
+}
+
+extern "C" int sbwt_search_reads_host_multi(sbwt_index *const *indexes, int n_indexes, const uint8_t *letters,
+                                            uint64_t n_letters, const uint64_t *row_starts, uint64_t n_rows,
+                                            uint64_t *answers, uint64_t n_kmers) {
+    clear_error();
+    if (!indexes || n_indexes < 1) return set_error("sbwt_search_reads_host_multi: no index");
+    for (int i = 0; i < n_indexes; i++) {
+        if (!indexes[i]) return set_error("index %d is NULL", i);
+        if (indexes[i]->k != indexes[0]->k || indexes[i]->n != indexes[0]->n || indexes[i]->C[4] != indexes[0]->C[4])
+            return set_error("index %d is not a replica of index 0", i);
+        for (int j = 0; j < i; j++)
+            if (indexes[j] == indexes[i]) return set_error("index %d is passed twice", i);
+    }
+    if (n_rows == 0) return 0;
+    if (!letters || !row_starts || (n_kmers && !answers)) return set_error("NULL host pointer");
+    const u32 k = indexes[0]->k;
+    std::vector<u64> bounds((size_t)n_indexes + 1);
+    SBWT_TRY(sbwt_partition_rows(row_starts, n_rows, k, n_indexes, bounds.data()));
+    // answers of part i start at the k-mers before its first row
+    std::vector<u64> k0((size_t)n_indexes + 1, 0);
+    for (int i = 0; i < n_indexes; i++) {
+        u64 nk = 0;
+        for (u64 r = bounds[i]; r < bounds[i + 1]; r++) {
+            const u64 len = row_starts[r + 1] - row_starts[r];
+            nk += len >= k ? len - k + 1 : 0;
+        }
+        k0[i + 1] = k0[i] + nk;
+    }
+    if (k0[n_indexes] != n_kmers)
+        return set_error("n_kmers = %llu but the rows hold %llu k-mers", (unsigned long long)n_kmers,
+                         (unsigned long long)k0[n_indexes]);
+    // host threads: the OpenMP threads of this call shared among the replicas (unless set per index)
+    const int share = std::max(1, omp_get_max_threads() / n_indexes);
+    std::vector<int> rc((size_t)n_indexes, 0);
+    std::vector<std::string> err((size_t)n_indexes);
+    std::vector<std::thread> th;
+    for (int i = 0; i < n_indexes; i++) {
+        th.emplace_back([&, i] {
+            sbwt_index *ix = indexes[i];
+            const int saved = ix->host_threads;
+            if (saved == 0) ix->host_threads = share;
+            rc[i] = run_pipeline(ix, letters, n_letters, row_starts + bounds[i], bounds[i + 1] - bounds[i],
+                                 answers ? answers + k0[i] : nullptr, nullptr, k0[i + 1] - k0[i]);
+            if (rc[i]) err[i] = last_error();
+            ix->host_threads = saved;
+        });
+    }
+    for (auto &t : th) t.join();
+    for (int i = 0; i < n_indexes; i++)
+        if (rc[i]) return set_error("replica %d (device %d): %s", i, indexes[i]->device, err[i].c_str());
+    return 0;
 }

@@ -195,6 +195,16 @@ def haplotypes(rng, base, n, snp=0.005, indel=0.0005, indel_max=20):
     return out
 
 
+def write_fastq(path, letters, row_starts, crlf=False):
+    """Writes rows as FASTQ records (@header, sequence, '+', qualities of the same length)."""
+    rs = np.asarray(row_starts, dtype=np.int64)
+    eol = b"\r\n" if crlf else b"\n"
+    with open(path, "wb") as f:
+        for i in range(rs.size - 1):
+            seq = letters[rs[i]:rs[i + 1]].tobytes()
+            f.write(b"@r%d length=%d" % (i, len(seq)) + eol + seq + eol + b"+" + eol + b"I" * len(seq) + eol)
+
+
 def write_fasta(path, letters, row_starts, width=None):
     """Writes rows as FASTA records (one header + one sequence line each, '\\n'-terminated)."""
     rs = np.asarray(row_starts, dtype=np.int64)

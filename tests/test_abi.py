@@ -112,3 +112,70 @@ def test_read_queries_many_concatenates(tmp_path):
         assert np.array_equal(rows[r0:r1 + 1] - rows[r0], p[1])
     with pytest.raises(sg.SbwtError):
         sg.read_queries_many(paths + [str(tmp_path / "missing.fa")], 31)
+
+
+def _reads(n=40, seed=5):
+    rng = wl.rng_for(seed)
+    g = wl.random_bases(rng, 5000)
+    letters, rows = wl.mixed_reads(rng, g, n // 2, n - n // 2, 60, 0.01)
+    lens = np.diff(rows.astype(np.int64))
+    lens[::7] = np.minimum(lens[::7], 20)  # some reads shorter than k
+    parts = [letters[int(rows[i]):int(rows[i]) + int(lens[i])] for i in range(lens.size)]
+    letters = np.concatenate(parts)
+    rows = np.zeros(lens.size + 1, dtype=np.uint64)
+    rows[1:] = np.cumsum(lens)
+    return letters, rows
+
+
+@pytest.mark.parametrize("crlf", [False, True])
+def test_fastq_reads_equal_the_fasta_reads(tmp_path, crlf):
+    """A FASTQ file (first byte '@') is read as four-line records whose sequence lines are the reads:
+    the same letters and rows as the FASTA file of the same reads (no reference counterpart; the
+    reference reads FASTA only)."""
+    letters, rows = _reads()
+    fq, fa = str(tmp_path / "q.fq"), str(tmp_path / "q.fa")
+    wl.write_fastq(fq, letters, rows)
+    wl.write_fasta(fa, letters, rows)
+    a = sg.read_queries(fq, 31)
+    b = sg.read_queries(fa, 31)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]
+    if crlf:  # CR LF line ends: the CR stays a letter of the read, as in the FASTA reading
+        wl.write_fastq(fq, letters, rows, crlf=True)
+        lt, rw, _ = sg.read_queries(fq, 31)
+        assert rw.size == rows.size and lt.size == letters.size + rows.size - 1
+        assert lt[int(rw[1]) - 1] == ord("\r")
+
+
+@pytest.mark.parametrize("fmt", ["fasta", "fastq"])
+@pytest.mark.parametrize("max_letters", [1, 333, 1000, 10_000_000])
+def test_streamed_batches_concatenate_to_the_whole_file(tmp_path, fmt, max_letters):
+    """sbwt_reader_next hands out batches of whole reads of at most max_letters letters (one longer read
+    alone); concatenated, they are exactly the whole-file reading."""
+    letters, rows = _reads(200, seed=6)
+    path = str(tmp_path / ("q.fq" if fmt == "fastq" else "q.fa"))
+    (wl.write_fastq if fmt == "fastq" else wl.write_fasta)(path, letters, rows)
+    whole = sg.read_queries(path, 31)
+    got_l, got_lens, nk = [], [], 0
+    for lt, rw, k in sg.read_query_batches(path, 31, max_letters):
+        assert rw.size >= 2 and (lt.size <= max_letters or rw.size == 2)
+        got_l.append(lt)
+        got_lens.append(np.diff(rw.astype(np.int64)))
+        nk += k
+    assert np.array_equal(np.concatenate(got_l), whole[0])
+    assert np.array_equal(np.concatenate(got_lens), np.diff(whole[1].astype(np.int64)))
+    assert nk == whole[2]
+
+
+def test_malformed_and_truncated_fastq(tmp_path):
+    bad = tmp_path / "bad.fq"
+    bad.write_bytes(b"@r0\nACGTACGT\nX\nIIIIIIII\n")  # the third line must start with '+'
+    with pytest.raises(sg.SbwtError, match="not FASTQ"):
+        sg.read_queries(str(bad), 5)
+    cut = tmp_path / "cut.fq"
+    cut.write_bytes(b"@r0\nACGTACGT\n+\nIIIIIIII\n@r1\nACGT\n")
+    with pytest.raises(sg.SbwtError, match="ends inside a FASTQ record"):
+        sg.read_queries(str(cut), 5)
+    ok = tmp_path / "ok.fq"
+    ok.write_bytes(b"@r0\nACGTACGT\n+\nIIIIIIII\n@r1\nACGT\n+\nIIII")  # no final newline
+    lt, rw, nk = sg.read_queries(str(ok), 5)
+    assert lt.tobytes() == b"ACGTACGTACGT" and rw.tolist() == [0, 8, 12] and nk == 4

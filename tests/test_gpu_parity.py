@@ -262,6 +262,33 @@ def test_small_workload_full(cuda, tmp_path):
         assert hashlib.sha256(text).hexdigest() == json.load(open(meta_p))["reference_sha256"]
 
 
+@pytest.mark.parametrize("fmt,batch", [("fasta", 0), ("fastq", 0), ("fastq", 100_000), ("fasta", 77_777)])
+def test_cli_streams_fasta_and_fastq(cuda, tmp_path, fmt, batch):
+    """The CLI reads its query file on a thread of its own in batches of whole reads while the
+    previous batch is searched; FASTQ input (no reference counterpart) gives the same output as the
+    FASTA file of the same reads.  On the small workload (1.2M k-mers), over up to ~20 batches, the
+    output's SHA-256 equals that of the reference program's output on the FASTA file."""
+    import make_golden
+    n, letters, rows = make_golden.write_small_workload(str(tmp_path))
+    q = str(tmp_path / "queries.fa")
+    if fmt == "fastq":
+        q = str(tmp_path / "queries.fq")
+        wl.write_fastq(q, letters, rows)
+    flags = [f if not f.startswith("--file-queries=") else f"--file-queries={q}"
+             for f in make_golden.small_workload_flags(str(tmp_path))]
+    env = dict(os.environ)
+    if batch:
+        env["SBWT_CLI_BATCH_LETTERS"] = str(batch)
+    r = subprocess.run([sg.CLI_PATH] + flags, capture_output=True, timeout=300, env=env)
+    assert r.returncode == 0, r.stderr.decode()
+    want = orc.format_answers(rows, 31, orc.OracleIndex.from_files([str(tmp_path / f"ix.{c}") for c in "ACGT"])
+                              .search_reads(letters, rows, 31, 10))
+    assert r.stdout == want
+    meta_p = os.path.join(GOLDEN, "small_workload.json")
+    if os.path.exists(meta_p):
+        assert hashlib.sha256(r.stdout).hexdigest() == json.load(open(meta_p))["reference_sha256"]
+
+
 @pytest.mark.parametrize("case", CASES)
 def test_cli_matches_reference_program(case, cuda):
     d = os.path.join(GOLDEN, "cases", case)
@@ -307,9 +334,18 @@ def test_autotune_keeps_answers_and_picks_a_shape(small, cuda):
         d_ans = torch.empty(want.size, dtype=torch.int64, device=cuda)
         rep = ix.autotune(_t(small["letters"], cuda), _t(small["rows"], cuda), d_ans, want.size, tune_p=True,
                           tune_poppy=True)
-        assert rep["best"]["ms"] > 0 and len(rep["candidates"]) >= 37
+        assert rep["best"]["ms"] > 0 and rep["default_ms"] > 0 and len(rep["candidates"]) >= 15
+        layouts = {c["layout"] for c in rep["candidates"]}
+        assert {"lines", "lines512", "lines2048", "poppy"} <= layouts
+        assert {c["window"] for c in rep["candidates"]} >= {64, 128, 256}
+        assert {c["p"] for c in rep["candidates"]} >= {8, 10, 12, 14}
         got = run_reads(ix, small["letters"], small["rows"], cuda)
+        # with the per-k-mer kernel's register shapes as well
+        rep2 = ix.autotune(_t(small["letters"], cuda), _t(small["rows"], cuda), d_ans, want.size, tune_shapes=True)
+        assert sum(1 for c in rep2["candidates"] if c["kmers_per_thread"] > 0) >= 36
+        got2 = run_reads(ix, small["letters"], small["rows"], cuda)
     assert np.array_equal(got, want)
+    assert np.array_equal(got2, want)
 
 
 def test_graph_replay_matches(small, cuda):
@@ -506,7 +542,7 @@ def test_host_pipelines_across_chunks(small, cuda):
     assert np.array_equal(mem, _bits_of(want))
 
 
-@pytest.mark.parametrize("transfer", ["sparse", "dense", "hybrid"])
+@pytest.mark.parametrize("transfer", ["sparse", "dense", "hybrid", "threads2"])
 @pytest.mark.parametrize("chunk", [4096, 50_000])
 def test_host_answers_sparse_transfer_many_chunks(small, cuda, monkeypatch, chunk, transfer):
     """The host answers pipeline brings a chunk's answers back as its membership bitmap, group
@@ -537,16 +573,24 @@ def test_host_answers_sparse_transfer_many_chunks(small, cuda, monkeypatch, chun
     rows[1:] = np.cumsum([p.size for p in parts])
     want = orc.OracleIndex(b.bits, b.n_bits).search_reads(letters, rows, k, 10)
     monkeypatch.setenv("SBWT_PIPELINE_CHUNK_LETTERS", str(chunk))
-    monkeypatch.setenv("SBWT_PIPELINE_TRANSFER", transfer)
+    if transfer == "threads2":  # two host threads: the split by sbwt_pipeline_dense_share (72 % of chunks dense)
+        monkeypatch.delenv("SBWT_PIPELINE_TRANSFER", raising=False)
+    else:
+        monkeypatch.setenv("SBWT_PIPELINE_TRANSFER", transfer)
     with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=10) as ix:
+        if transfer == "threads2":
+            ix.set_host_threads(2)
         host = ix.search_reads_host(letters, rows)
         moved = ix.pipeline_bytes()
         pa = torch.empty(want.size, dtype=torch.int64).pin_memory()  # hybrid copies into pinned buffers
         ix.search_reads_host(letters, rows, pa)
+        moved_pinned = ix.pipeline_bytes()
         mem = ix.member_reads_host(letters, rows)
     assert letters.size > 2 * chunk
     assert moved["h2d"] > letters.size and 0 < moved["d2h"]
     assert (moved["d2h"] >= 8 * want.size) == (transfer == "dense")
+    if transfer == "threads2":  # the pinned call sent most answers dense, some sparse
+        assert 0.25 * 8 * want.size < moved_pinned["d2h"] < 8 * want.size
     assert np.array_equal(pa.numpy().view(np.uint64), want)
     assert (want != orc.NOT_FOUND).mean() > 0.3 and (want == orc.NOT_FOUND).any()
     assert np.array_equal(host, want)

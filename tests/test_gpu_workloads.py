@@ -70,3 +70,33 @@ def test_pangenome_union_index(cuda):
     assert (got[:n_pos] != orc.NOT_FOUND).all()  # every haplotype k-mer is indexed
     sub_hits = (got[n_pos:n_pos + subs.shape[0] * 120] != orc.NOT_FOUND).mean()
     assert 0.2 < sub_hits < 0.95  # substituted reads mix found and absent k-mers
+
+
+def test_search_reads_host_multi_replicas(cuda):
+    """sbwt_search_reads_host_multi: the rows split into contiguous ranges of near-equal k-mer counts, one
+    index replica per range, each writing its own slice of the answers.  Only one GPU is visible here, so
+    the replicas share it (their pipelines are independent: no replica waits on another); the answers
+    equal the oracle's for 1, 2 and 3 replicas, and a non-replica is refused."""
+    rng = wl.rng_for(61)
+    genome = wl.random_bases(rng, 150_000)
+    built = sg.build_sbwt([genome.tobytes()], 31)
+    files = list(wl.uneven_read_files(genome, seed=62, total_kmers=600_000, n_files=4))
+    letters = np.concatenate([lt for lt, _ in files])
+    rows, off = [np.zeros(1, dtype=np.uint64)], 0
+    for lt, rw in files:
+        rows.append(rw[1:].astype(np.uint64) + np.uint64(off))
+        off += lt.size
+    rows = np.concatenate(rows)
+    want = orc.OracleIndex(built.bits, built.n_bits).search_reads(letters, rows, 31, 10)
+    ixs = [sg.Index.from_bits(built.bits, built.n_bits, k=31, k_presearch=10) for _ in range(3)]
+    try:
+        for n in (1, 2, 3):
+            got = sg.search_reads_host_multi(ixs[:n], letters, rows)
+            assert np.array_equal(got, want), n
+        other = sg.build_sbwt([genome[:50_000].tobytes()], 31)
+        with sg.Index.from_bits(other.bits, other.n_bits, k=31, k_presearch=10) as bad:
+            with pytest.raises(sg.SbwtError, match="not a replica"):
+                sg.search_reads_host_multi([ixs[0], bad], letters, rows)
+    finally:
+        for ix in ixs:
+            ix.close()

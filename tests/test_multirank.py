@@ -91,3 +91,55 @@ def test_host_threads_per_rank(monkeypatch):
         monkeypatch.setenv("LOCAL_WORLD_SIZE", str(local))
         b.host_threads_per_rank(world, impl)
         assert os.environ["OMP_NUM_THREADS"] == want, (impl, world, env)
+
+
+def test_answer_transfer_degrades_with_the_per_rank_thread_split(monkeypatch):
+    """Under torchrun each rank of this project's arm gets cores / ranks host threads; with 8 ranks on a
+    16-core node that is 2.  The host pipeline then sends the share of chunks that lets the copy engines
+    and the 2 expanding threads finish together as u64 answers (72 %), not every chunk (the all-dense form,
+    PCIe-bound) and not none (2 threads would expand far slower than PCIe copies)."""
+    import bench as b
+    import sbwt_gpu_b200 as sg
+    monkeypatch.delenv("SBWT_PIPELINE_TRANSFER", raising=False)
+    n = 100_200_000  # the large workload's columns
+    monkeypatch.setenv("OMP_NUM_THREADS", "1")  # what torchrun sets
+    monkeypatch.setenv("LOCAL_WORLD_SIZE", "8")
+    monkeypatch.setattr(os, "sched_getaffinity", lambda pid: set(range(16)))
+    b.host_threads_per_rank(8, "ours")
+    t = int(os.environ["OMP_NUM_THREADS"])
+    assert t == 2
+    f = sg.pipeline_dense_share(n, t)
+    assert 0.6 < f < 0.8
+    # the modelled time of the split is below both pure forms: dense DMA 57 GB/s, expansion 11 GB/s a thread
+    dense_t, expand_t = 1 / 57.0, 1 / (11.0 * t)
+    split_t = max(f * dense_t, (1 - f) * expand_t)
+    assert split_t < 0.8 * dense_t and split_t < expand_t
+    # more threads: all sparse; fewer: a larger dense share; indexes past 2^32 columns: all dense
+    assert sg.pipeline_dense_share(n, 16) == 0.0 and sg.pipeline_dense_share(n, 6) == 0.0
+    assert sg.pipeline_dense_share(n, 1) > f > sg.pipeline_dense_share(n, 4) > 0.0
+    assert sg.pipeline_dense_share(1 << 33, 16) == 1.0
+    monkeypatch.setenv("SBWT_PIPELINE_TRANSFER", "sparse")
+    assert sg.pipeline_dense_share(n, 2) == 0.0
+
+
+@pytest.mark.parametrize("n_parts", [1, 2, 3, 4, 8])
+def test_partition_rows_balances_kmers_and_never_splits_a_row(n_parts):
+    """sbwt_partition_rows (the split of sbwt_search_reads_host_multi, one range per GPU): contiguous
+    ranges covering every row once, each within one row's k-mers of an equal share."""
+    import numpy as np
+    import sbwt_gpu_b200 as sg
+    rng = np.random.default_rng(n_parts)
+    k = 31
+    lens = rng.choice([0, 10, 31, 150, 151, 2000, 15_000], size=5000, p=[.05, .05, .05, .6, .1, .1, .05])
+    rows = np.zeros(lens.size + 1, dtype=np.uint64)
+    rows[1:] = np.cumsum(lens)
+    b = sg.partition_rows(rows, k, n_parts).astype(np.int64)
+    assert b[0] == 0 and b[-1] == lens.size and (np.diff(b) >= 0).all()
+    per_row = np.maximum(lens - k + 1, 0)
+    counts = np.array([per_row[b[i]:b[i + 1]].sum() for i in range(n_parts)])
+    assert counts.sum() == per_row.sum()
+    assert np.abs(counts - per_row.sum() / n_parts).max() <= per_row.max()
+    # a batch with fewer rows than parts: empty ranges, nothing lost
+    few = np.array([0, 200, 400], dtype=np.uint64)
+    bf = sg.partition_rows(few, k, 4).astype(np.int64)
+    assert bf[0] == 0 and bf[-1] == 2 and (np.diff(bf) >= 0).all()
