@@ -99,7 +99,11 @@ __global__ void __launch_bounds__(128) gemm_tn_kernel(const bf16 *__restrict__ A
 
 // --------------------------------------------------------- fused inference
 
-constexpr u32 kInferSmem = kHid * kIn * 2 + kHid * kHid * 2 + kTileM * kIn * 2;  // 224 KiB
+// W1, W2, the one-hot tile and the per-column-group partial dots: 226 KiB
+constexpr u32 kInferThreads = 512;
+constexpr u32 kColGroups = kInferThreads / kTileM;  // 4
+constexpr u32 kGroupCols = kHid / kColGroups;       // 64
+constexpr u32 kInferSmem = kHid * kIn * 2 + kHid * kHid * 2 + kTileM * kIn * 2 + kColGroups * kTileM * 4;
 
 // One-hot chunks q0..q1-1 of row r: chunk q holds inputs 8q..8q+7 = letters
 // 2q and 2q+1 (4 one-hot inputs each).
@@ -119,32 +123,88 @@ __device__ __forceinline__ void onehot_chunks(uint8_t *tile, u32 R, u32 r, u64 k
     }
 }
 
-// One CTA per SM (224 KiB of shared memory, all 512 TMEM columns), 512
+// One CTA per SM (226 KiB of shared memory, all 512 TMEM columns), 512
 // threads = 16 warps.  b1, b2 and w3 must be 16-byte aligned (float4 loads;
-// their offsets in the parameter vector are multiples of 4 floats).  Warp w reaches TMEM lanes 32*(w%4)..+31 (rows of the
-// 128-k-mer tile) and handles hidden columns 64*(w/4)..+63 of them in both
-// epilogues, so four warps share each row and the epilogues run on all 16
-// warps; layer 2's 256 -> 1 dot is summed over the four column groups in
-// shared memory (the one-hot tile's space, free once layer 1 has run).
-constexpr u32 kInferThreads = 512;
-constexpr u32 kColGroups = kInferThreads / kTileM;  // 4
-constexpr u32 kGroupCols = kHid / kColGroups;       // 64
+// their offsets in the parameter vector are multiples of 4 floats).  Warp w
+// reaches TMEM lanes 32*(w%4)..+31 (rows of the 128-k-mer tile) and handles
+// hidden columns 64*(w/4)..+63 of them in both epilogues, so four warps
+// share each row and the epilogues run on all 16 warps; layer 2's 256 -> 1
+// dot is summed over the four column groups in shared memory.
+//
+// Pipelined over tiles with the TMEM columns in two halves of 256: tile t
+// accumulates in half h (layer 1, then layer 2 over it) and keeps its
+// layer-1 activations (layer 2's A operand, BF16 pairs) in the first 128
+// columns of the other half.  Once layer 2 of tile t has run, that other
+// half is free, so tile t+1's layer-1 MMA runs there while the threads do
+// tile t's layer-2 epilogue, and tile t+1's one-hot tile is built while
+// tile t's layer-2 MMA runs:
+//   epi1(t) -> MMA2(t) || one-hot(t+1) -> MMA1(t+1) || epi2(t) -> epi1(t+1) ...
+// Two mbarriers (layer 1, layer 2), each with its own phase.
+__device__ __forceinline__ void infer_epi1(u32 tacc, u32 ta2, u32 lane_base, u32 c0, const float *__restrict__ b1) {
+    u32 v[4][16];
+#pragma unroll
+    for (u32 j = 0; j < 4; j++) tmem_ld16(tacc + lane_base + c0 + 16u * j, v[j]);
+    tmem_wait_ld();
+#pragma unroll
+    for (u32 j = 0; j < 4; j++) {
+        tmem_tie(v[j]);
+        u32 packed[8];
+#pragma unroll
+        for (int t = 0; t < 16; t += 4) {
+            // the same 4 biases for every lane of the warp: one 16-byte load
+            const float4 bb = __ldg(reinterpret_cast<const float4 *>(b1 + c0 + 16u * j + t));
+            packed[t / 2] = pack_bf16x2(fmaxf(__uint_as_float(v[j][t]) + bb.x, 0.0f),
+                                        fmaxf(__uint_as_float(v[j][t + 1]) + bb.y, 0.0f));
+            packed[t / 2 + 1] = pack_bf16x2(fmaxf(__uint_as_float(v[j][t + 2]) + bb.z, 0.0f),
+                                            fmaxf(__uint_as_float(v[j][t + 3]) + bb.w, 0.0f));
+        }
+        tmem_st8(ta2 + lane_base + (c0 + 16u * j) / 2u, packed);
+    }
+    tmem_wait_st();
+}
+
+// Partial dot of one row's 64 layer-2 activations (bias, ReLU, BF16) with w3.
+__device__ __forceinline__ float infer_epi2(u32 tacc, u32 lane_base, u32 c0, const float *__restrict__ b2,
+                                            const float *__restrict__ w3) {
+    u32 v[4][16];
+#pragma unroll
+    for (u32 j = 0; j < 4; j++) tmem_ld16(tacc + lane_base + c0 + 16u * j, v[j]);
+    tmem_wait_ld();
+    float acc = 0.0f;
+#pragma unroll
+    for (u32 j = 0; j < 4; j++) {
+        tmem_tie(v[j]);
+#pragma unroll
+        for (int t = 0; t < 16; t += 4) {
+            const u32 c = c0 + 16u * j + t;
+            const float4 bb = __ldg(reinterpret_cast<const float4 *>(b2 + c));
+            const float4 ww = __ldg(reinterpret_cast<const float4 *>(w3 + c));
+            acc = fmaf(bf16_round(fmaxf(__uint_as_float(v[j][t]) + bb.x, 0.0f)), ww.x, acc);
+            acc = fmaf(bf16_round(fmaxf(__uint_as_float(v[j][t + 1]) + bb.y, 0.0f)), ww.y, acc);
+            acc = fmaf(bf16_round(fmaxf(__uint_as_float(v[j][t + 2]) + bb.z, 0.0f)), ww.z, acc);
+            acc = fmaf(bf16_round(fmaxf(__uint_as_float(v[j][t + 3]) + bb.w, 0.0f)), ww.w, acc);
+        }
+    }
+    return acc;
+}
 
 __global__ void __launch_bounds__(kInferThreads, 1)
     mlp_infer_kernel(const u64 *__restrict__ kmers, u64 n, u32 k, const bf16 *__restrict__ W1b,
                      const bf16 *__restrict__ W2b, const float *__restrict__ b1, const float *__restrict__ b2,
                      const float *__restrict__ w3, const float *__restrict__ b3, const InferOut out, int *err) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ uint64_t bar;
+    __shared__ uint64_t bar1, bar2;
     __shared__ u32 tmem_s;
     uint8_t *sW1 = smem;
     uint8_t *sW2 = smem + kHid * kIn * 2;
     uint8_t *sX = sW2 + kHid * kHid * 2;
-    float *sRed = reinterpret_cast<float *>(sX);  // [kColGroups][kTileM] partial dots (after layer 1)
+    float *sRed = reinterpret_cast<float *>(sX + kTileM * kIn * 2);  // [kColGroups][kTileM] partial dots
     const u32 tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
     const u32 quarter = warp & 3u, cg = warp >> 2;
     const u32 trow = quarter * 32u + lane;  // this thread's row of the tile
     const u32 c0 = cg * kGroupCols;         // its first hidden column
+    const u32 xr = tid & (kTileM - 1u), xg = tid / kTileM;  // one-hot: row, chunk group
+    constexpr u32 kChunks = kIn / 8 / kColGroups;             // 4 of the 16 chunks of a row
     // weights into the canonical K-major layouts (once per launch)
     for (u32 i = tid; i < kHid * (kIn / 8); i += kInferThreads) {
         const u32 r = i / (kIn / 8), kc = i % (kIn / 8);
@@ -157,68 +217,48 @@ __global__ void __launch_bounds__(kInferThreads, 1)
             *reinterpret_cast<const uint4 *>(W2b + (size_t)r * kHid + kc * 8);
     }
     if (warp == 0) tmem_alloc(&tmem_s, 512);
-    if (tid == 0) mbar_init(&bar, 1);
+    if (tid == 0) {
+        mbar_init(&bar1, 1);
+        mbar_init(&bar2, 1);
+    }
+    // the first tile's one-hot tile
+    u64 tile = blockIdx.x;
+    {
+        const u64 row = tile * kTileM + xr;
+        onehot_chunks(sX, kTileM, xr, row < n ? kmers[row] : 0ull, k, xg * kChunks, (xg + 1) * kChunks);
+    }
+    fence_smem_to_async();
     fence_before_sync();
     __syncthreads();
     fence_after_sync();
-    const u32 tD = tmem_s;          // columns [0, 256): layer accumulators
-    const u32 tA2 = tmem_s + 256u;  // columns [256, 384): layer-1 activations, BF16 pairs
+    const u32 T0 = tmem_s;
     const u32 lane_base = (quarter * 32u) << 16;
     const float bias3 = __ldg(b3);
-    u32 phase = 0;
-    bool ok = true;
-    // one-hot tile: thread (row tid % 128, chunk group tid / 128); the k-mer of
-    // the next tile is loaded while this tile's layer-1 MMA runs
-    const u32 xr = tid & (kTileM - 1u), xg = tid / kTileM;
-    u64 kmer = (u64)blockIdx.x * kTileM + xr < n ? kmers[(u64)blockIdx.x * kTileM + xr] : 0ull;
-    for (u64 tile = blockIdx.x; ok && tile * kTileM < n; tile += gridDim.x) {
-        {
-            constexpr u32 kChunks = kIn / 8 / kColGroups;  // 4 of the 16 chunks of a row
-            onehot_chunks(sX, kTileM, xr, kmer, k, xg * kChunks, (xg + 1) * kChunks);
-        }
-        fence_smem_to_async();
-        __syncthreads();
-        if (tid == 0) {
-            fence_after_sync();
+    auto mma1 = [&](u32 tacc) {  // layer 1: one-hot tile x W1^T into tacc (thread 0, after a thread sync)
+        fence_after_sync();
 #pragma unroll
-            for (u32 s = 0; s < kIn / 16; s++) {
-                const u64 da = smem_desc(smem_addr(sX) + s * 2u * kTileM * 16u, kTileM * 16u, 128u);
-                const u64 db = smem_desc(smem_addr(sW1) + s * 2u * kHid * 16u, kHid * 16u, 128u);
-                mma_ss(tD, da, db, idesc_bf16(kTileM, kHid), s > 0);
-            }
-            mma_commit(&bar);
+        for (u32 s = 0; s < kIn / 16; s++) {
+            const u64 da = smem_desc(smem_addr(sX) + s * 2u * kTileM * 16u, kTileM * 16u, 128u);
+            const u64 db = smem_desc(smem_addr(sW1) + s * 2u * kHid * 16u, kHid * 16u, 128u);
+            mma_ss(tacc, da, db, idesc_bf16(kTileM, kHid), s > 0);
         }
-        {
-            const u64 nrow = (tile + gridDim.x) * kTileM + xr;
-            kmer = nrow < n ? kmers[nrow] : 0ull;
-        }
-        bool got = mbar_wait(&bar, phase, err, kErrInferWait1);
-        phase ^= 1u;
+        mma_commit(&bar1);
+    };
+    u32 ph1 = 0, ph2 = 0;
+    bool pend1 = false, pend2 = false;  // an MMA commit outstanding on bar1 / bar2
+    bool ok = true;
+    u32 half = 0;  // this tile accumulates in columns [256 half, +256), its A2 at the other half
+    if (tid == 0) mma1(T0);
+    pend1 = true;
+    for (;;) {
+        const u32 tacc = T0 + 256u * half, ta2 = T0 + 256u * (half ^ 1u);
+        // ---- layer 1 done: bias, ReLU, BF16 into the other half's first 128 columns
+        bool got = mbar_wait(&bar1, ph1, err, kErrInferWait1);
+        ph1 ^= 1u;
+        pend1 = false;
         fence_after_sync();
         if (!__syncthreads_and(got)) { ok = false; break; }
-        // layer-1 epilogue on this thread's 64 columns: bias, ReLU, BF16, into TMEM as layer 2's A
-        {
-            u32 v[4][16];
-#pragma unroll
-            for (u32 j = 0; j < 4; j++) tmem_ld16(tD + lane_base + c0 + 16u * j, v[j]);
-            tmem_wait_ld();
-#pragma unroll
-            for (u32 j = 0; j < 4; j++) {
-                tmem_tie(v[j]);
-                u32 packed[8];
-#pragma unroll
-                for (int t = 0; t < 16; t += 4) {
-                    // the same 4 biases for every lane of the warp: one 16-byte load
-                    const float4 bb = __ldg(reinterpret_cast<const float4 *>(b1 + c0 + 16u * j + t));
-                    packed[t / 2] = pack_bf16x2(fmaxf(__uint_as_float(v[j][t]) + bb.x, 0.0f),
-                                                fmaxf(__uint_as_float(v[j][t + 1]) + bb.y, 0.0f));
-                    packed[t / 2 + 1] = pack_bf16x2(fmaxf(__uint_as_float(v[j][t + 2]) + bb.z, 0.0f),
-                                                    fmaxf(__uint_as_float(v[j][t + 3]) + bb.w, 0.0f));
-                }
-                tmem_st8(tA2 + lane_base + (c0 + 16u * j) / 2u, packed);
-            }
-        }
-        tmem_wait_st();
+        infer_epi1(tacc, ta2, lane_base, c0, b1);
         fence_before_sync();
         __syncthreads();
         if (tid == 0) {
@@ -226,37 +266,32 @@ __global__ void __launch_bounds__(kInferThreads, 1)
 #pragma unroll
             for (u32 s = 0; s < kHid / 16; s++) {
                 const u64 db = smem_desc(smem_addr(sW2) + s * 2u * kHid * 16u, kHid * 16u, 128u);
-                mma_ts(tD, tA2 + s * 8u, db, idesc_bf16(kTileM, kHid), s > 0);
+                mma_ts(tacc, ta2 + s * 8u, db, idesc_bf16(kTileM, kHid), s > 0);
             }
-            mma_commit(&bar);
+            mma_commit(&bar2);
         }
-        got = mbar_wait(&bar, phase, err, kErrInferWait2);
-        phase ^= 1u;
+        pend2 = true;
+        // ---- while layer 2 runs: the next tile's one-hot tile (layer 1 has read this one)
+        const u64 next = tile + gridDim.x;
+        const bool has_next = next * kTileM < n;
+        if (has_next) {
+            const u64 row = next * kTileM + xr;
+            onehot_chunks(sX, kTileM, xr, row < n ? kmers[row] : 0ull, k, xg * kChunks, (xg + 1) * kChunks);
+        }
+        fence_smem_to_async();
+        got = mbar_wait(&bar2, ph2, err, kErrInferWait2);
+        ph2 ^= 1u;
+        pend2 = false;
         fence_after_sync();
         if (!__syncthreads_and(got)) { ok = false; break; }
-        // layer-2 epilogue: bias, ReLU, BF16 activation, partial dot with w3 over 64 columns
-        {
-            u32 v[4][16];
-#pragma unroll
-            for (u32 j = 0; j < 4; j++) tmem_ld16(tD + lane_base + c0 + 16u * j, v[j]);
-            tmem_wait_ld();
-            float acc = 0.0f;
-#pragma unroll
-            for (u32 j = 0; j < 4; j++) {
-                tmem_tie(v[j]);
-#pragma unroll
-                for (int t = 0; t < 16; t += 4) {
-                    const u32 c = c0 + 16u * j + t;
-                    const float4 bb = __ldg(reinterpret_cast<const float4 *>(b2 + c));
-                    const float4 ww = __ldg(reinterpret_cast<const float4 *>(w3 + c));
-                    acc = fmaf(bf16_round(fmaxf(__uint_as_float(v[j][t]) + bb.x, 0.0f)), ww.x, acc);
-                    acc = fmaf(bf16_round(fmaxf(__uint_as_float(v[j][t + 1]) + bb.y, 0.0f)), ww.y, acc);
-                    acc = fmaf(bf16_round(fmaxf(__uint_as_float(v[j][t + 2]) + bb.z, 0.0f)), ww.z, acc);
-                    acc = fmaf(bf16_round(fmaxf(__uint_as_float(v[j][t + 3]) + bb.w, 0.0f)), ww.w, acc);
-                }
-            }
-            sRed[cg * kTileM + trow] = acc;
+        // ---- layer 2 done: the next tile's layer 1 into the other half (this tile's A2 is spent)
+        if (has_next) {
+            if (tid == 0) mma1(ta2);
+            pend1 = true;
         }
+        // ---- this tile's layer-2 epilogue while the next tile's layer 1 runs
+        sRed[cg * kTileM + trow] = infer_epi2(tacc, lane_base, c0, b2, w3);
+        fence_before_sync();
         __syncthreads();
         if (cg == 0) {
             const u64 row = tile * kTileM + trow;
@@ -274,11 +309,17 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                 if (lane == 0 && first < n) out.reject[first >> 5] = bits;
             }
         }
-        fence_before_sync();
+        // sRed is reused and this half's columns take the next tile's A2 only after every thread is here
         __syncthreads();
         fence_after_sync();
+        if (!has_next) break;
+        tile = next;
+        half ^= 1u;
     }
-    if (!ok && tid == 0) mbar_wait(&bar, phase ^ 1u, err, kErrInferWait2);
+    if (!ok && tid == 0) {  // let the MMAs still in flight land before the columns are freed
+        if (pend1) mbar_wait(&bar1, ph1, err, kErrInferWait1);
+        if (pend2) mbar_wait(&bar2, ph2, err, kErrInferWait2);
+    }
     fence_before_sync();
     __syncthreads();
     if (warp == 0) tmem_dealloc(tmem_s, 512);
