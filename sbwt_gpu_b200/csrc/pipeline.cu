@@ -26,7 +26,7 @@
 #include <thread>
 #include <vector>
 #if defined(__x86_64__)
-#include <emmintrin.h>
+#include <immintrin.h>
 #endif
 
 #include <cub/cub.cuh>
@@ -171,11 +171,78 @@ __global__ void __launch_bounds__(32 * kGroupWarps) group_nodes_kernel(const uin
     for (u32 q = lane; q < o; q += 32u) dst[q] = b[q];
 }
 
+#if defined(__x86_64__)
+// The expansion of the groups [g0, g1) with 32-byte streaming stores: the
+// output is walked in 32-byte-aligned blocks of 4 answers (a block of 4
+// absent k-mers is one constant store), with single 8-byte streaming stores
+// for the unaligned head and the tail.  Host CPUs with AVX2 only.
+__attribute__((target("avx2"))) void expand_groups_avx2(u64 *answers, u64 nk, const uint32_t *member,
+                                                        const u64 *goff, const uint32_t *nodes, u64 g0, u64 g1) {
+    const u64 j0 = g0 * kGroupWords * 32u, j1 = std::min<u64>(g1 * kGroupWords * 32u, nk);
+    if (j0 >= j1) return;
+    u64 o = goff[g0];
+    auto bit = [&](u64 j) { return (member[j >> 5] >> (j & 31u)) & 1u; };
+    u64 j = j0;
+    // head: up to the first 32-byte boundary of the output
+    while (j < j1 && (reinterpret_cast<uintptr_t>(answers + j) & 31u)) {
+        const u32 b = bit(j);
+        store_stream(answers + j, b ? (u64)nodes[o] : ~0ull);
+        o += b;
+        j++;
+    }
+    const __m256i none = _mm256_set1_epi64x(-1);
+    for (; j + 4 <= j1; j += 4) {
+        // the 4 bits of k-mers j .. j+3 (they may straddle two bitmap words)
+        const u64 w = j >> 5;
+        const u32 sh = (u32)(j & 31u);
+        const u64 pair = (u64)member[w] | (sh > 28u ? (u64)member[w + 1] << 32 : 0ull);
+        const u32 m4 = (u32)(pair >> sh) & 15u;
+        __m256i v;
+        if (m4 == 0) {
+            v = none;
+        } else {
+            long long x[4];
+            for (u32 i = 0; i < 4; i++) {
+                const u32 b = (m4 >> i) & 1u;
+                x[i] = b ? (long long)nodes[o] : -1ll;
+                o += b;
+            }
+            v = _mm256_set_epi64x(x[3], x[2], x[1], x[0]);
+        }
+        _mm256_stream_si256(reinterpret_cast<__m256i *>(answers + j), v);
+    }
+    for (; j < j1; j++) {  // tail
+        const u32 b = bit(j);
+        store_stream(answers + j, b ? (u64)nodes[o] : ~0ull);
+        o += b;
+    }
+}
+
+bool host_has_avx2() {
+    static const bool yes = __builtin_cpu_supports("avx2");
+    return yes;
+}
+#endif
+
 // answers[j] for the nk k-mers of one chunk from its sparse form (streaming
 // stores: the answers are not read back by this thread).  nodes may be read
 // one element past the chunk's found ids (a select instead of a branch), so
 // its buffer has slack.
 void expand_answers(u64 *answers, u64 nk, const uint32_t *member, const u64 *goff, const uint32_t *nodes, int threads) {
+#if defined(__x86_64__)
+    if (host_has_avx2() && (reinterpret_cast<uintptr_t>(answers) & 7u) == 0) {
+        const u64 nw = (nk + 31) / 32, ng = (nw + kGroupWords - 1) / kGroupWords;
+#pragma omp parallel num_threads(threads) if (nk > (1u << 16))
+        {
+            // contiguous runs of groups per thread: contiguous output, aligned blocks inside
+            const u64 nt = (u64)omp_get_num_threads(), t = (u64)omp_get_thread_num();
+            const u64 per = (ng + nt - 1) / nt;
+            expand_groups_avx2(answers, nk, member, goff, nodes, std::min(ng, t * per), std::min(ng, (t + 1) * per));
+            store_fence();
+        }
+        return;
+    }
+#endif
     const u64 nw = (nk + 31) / 32, ng = (nw + kGroupWords - 1) / kGroupWords;
 #pragma omp parallel num_threads(threads) if (nk > (1u << 16))
     {
