@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "device.cuh"
@@ -158,7 +159,11 @@ int finish_index(sbwt_index *ix, const u64 *const words[4], const sbwt_params *p
     if (ix->C[4] != n)
         return set_error("the bit vectors are not an SBWT: 1 + total ones = %llu but n = %llu",
                          (unsigned long long)ix->C[4], (unsigned long long)n);
-    apply_shape(ix, prm);
+    {
+        const int persist = ix->shape.l2_persist;  // set from the environment in new_index
+        apply_shape(ix, prm);
+        ix->shape.l2_persist = persist;
+    }
     if (ix->shape.layout != SBWT_LAYOUT_POPPY && !ix->lines_ok) ix->shape.layout = SBWT_LAYOUT_POPPY;
     if (sbwt::wide_sectors(ix->shape.layout)) SBWT_TRY(sbwt::build_wide(ix, sbwt::wide_sectors(ix->shape.layout), s));
     SBWT_CHECK_CUDA(cudaEventRecord(ev[2], s));
@@ -170,7 +175,7 @@ int finish_index(sbwt_index *ix, const u64 *const words[4], const sbwt_params *p
     for (int i = 0; i < 4; i++) SBWT_CHECK_CUDA(cudaEventElapsedTime(&ix->build_ms[i], ev[i], ev[i + 1]));
     if (!want_poppy) ix->build_ms[1] = 0.0f;
     if (!ix->stream_ok) ix->build_ms[3] = 0.0f;
-    return 0;
+    return sbwt::l2_setaside_acquire(ix);
 }
 
 int new_index(const sbwt_params *prm, sbwt_index **out, sbwt_index **ix_out) {
@@ -190,6 +195,12 @@ int new_index(const sbwt_params *prm, sbwt_index **out, sbwt_index **ix_out) {
     int l2 = 0;
     cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, prm->device);
     ix->l2_bytes = l2 > 0 ? (uint64_t)l2 : 0;
+    int mp = 0, mw = 0;
+    cudaDeviceGetAttribute(&mp, cudaDevAttrMaxPersistingL2CacheSize, prm->device);
+    cudaDeviceGetAttribute(&mw, cudaDevAttrMaxAccessPolicyWindowSize, prm->device);
+    ix->l2_max_persist = mp > 0 ? (size_t)mp : 0;
+    ix->l2_max_window = mw > 0 ? (size_t)mw : 0;
+    if (const char *e = std::getenv("SBWT_L2_PERSIST")) ix->shape.l2_persist = std::atoi(e) != 0;
     *ix_out = ix;
     return 0;
 }
@@ -303,6 +314,7 @@ extern "C" int sbwt_index_load(const char *file_a, const char *file_c, const cha
 extern "C" void sbwt_index_free(sbwt_index *ix) {
     if (!ix) return;
     cudaSetDevice(ix->device);
+    sbwt::l2_setaside_release(ix);
     cudaFree(ix->d_bits);
     cudaFree(ix->d_lines);
     cudaFree(ix->d_wide);
@@ -429,6 +441,75 @@ extern "C" int sbwt_set_search_mode(sbwt_index *ix, int32_t mode) {
 }
 
 namespace sbwt {
+
+// The rank lines of the line layouts are the run walk's most reused data
+// (every rank-pair step reads one or two of them), but the answer stream and
+// the gathers from the presearch and backward tables (each larger than L2 on
+// the large workload) push them out: measured, the L2 hit rate of the walk
+// was 20-27 % and its DRAM reads 22-25 bytes per k-mer against 4.5 bytes of
+// gathers the tables need.  So the search launch carries an access-policy
+// window over the current layout's lines with the persisting property, and
+// the index sizes the device's persisting L2 set-aside to hold them (a CUDA
+// context limit, released again when the last index that asked for it is
+// freed).  Layouts larger than the set-aside (poppy, or lines beyond it) get
+// no window.
+namespace {
+std::mutex g_l2_mutex;
+constexpr int kL2Devices = 64;
+int g_l2_users[kL2Devices] = {0};   // live indexes holding the set-aside
+size_t g_l2_set[kL2Devices] = {0};  // its size: the largest any of them asked for
+}  // namespace
+
+bool l2_window(const sbwt_index *ix, cudaAccessPolicyWindow *w) {
+    if (!ix->shape.l2_persist || ix->l2_setaside == 0) return false;
+    const void *base = nullptr;
+    size_t bytes = 0;
+    if (ix->shape.layout == SBWT_LAYOUT_LINES && ix->lines_ok) {
+        base = ix->d_lines, bytes = 4ull * ix->lpc * sizeof(ulonglong4);
+    } else if (wide_sectors(ix->shape.layout) && ix->wide_s == wide_sectors(ix->shape.layout)) {
+        base = ix->d_wide, bytes = 4ull * ix->wide_lpc * ix->wide_s * sizeof(ulonglong4);
+    }
+    if (!base || bytes > ix->l2_max_window || bytes > ix->l2_max_persist) return false;
+    w->base_ptr = const_cast<void *>(base);
+    w->num_bytes = bytes;
+    w->hitRatio = bytes <= ix->l2_setaside ? 1.0f : (float)ix->l2_setaside / (float)bytes;
+    w->hitProp = cudaAccessPropertyPersisting;
+    w->missProp = cudaAccessPropertyStreaming;
+    return true;
+}
+
+int l2_setaside_acquire(sbwt_index *ix) {
+    if (!ix->lines_ok || ix->l2_max_persist == 0 || ix->device < 0 || ix->device >= kL2Devices) return 0;
+    // the largest line layout this index may search: the 32-byte lines
+    const size_t want = std::min<size_t>(4ull * ix->lpc * sizeof(ulonglong4), ix->l2_max_persist);
+    std::lock_guard<std::mutex> lk(g_l2_mutex);
+    const int d = ix->device;
+    const size_t need = std::max(want, g_l2_set[d]);
+    if (need != g_l2_set[d]) {
+        const cudaError_t e = cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, need);
+        if (e != cudaSuccess) {  // no set-aside (for example under MPS): search without the window
+            cudaGetLastError();
+            return 0;
+        }
+        g_l2_set[d] = need;
+    }
+    g_l2_users[d]++;
+    ix->l2_setaside = need;
+    return 0;
+}
+
+void l2_setaside_release(sbwt_index *ix) {
+    if (ix->l2_setaside == 0 || ix->device < 0 || ix->device >= kL2Devices) return;
+    std::lock_guard<std::mutex> lk(g_l2_mutex);
+    const int d = ix->device;
+    if (--g_l2_users[d] <= 0) {
+        g_l2_users[d] = 0;
+        cudaCtxResetPersistingL2Cache();
+        cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
+        g_l2_set[d] = 0;
+    }
+    ix->l2_setaside = 0;
+}
 
 void set_gather_policies(const sbwt_index *ix, SearchArgs &a) {
     const u64 half = ix->l2_bytes / 2;

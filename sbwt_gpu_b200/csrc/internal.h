@@ -74,6 +74,7 @@ struct KernelShape {
     u32 window = 128;        // k-mers per window (line layout: 64, 128 or 256)
     u32 blocks_per_sm = 0;   // resident blocks per SM of the persistent grid (0: as many as fit)
     int evict = 0;           // evict-first gathers: 0 = when a table exceeds half of L2, 1 = never, 2 = always
+    int l2_persist = 1;      // the rank lines of the search layout held in the L2 set-aside (l2_window)
 };
 
 // Device buffers of one in-flight search (grow-only).
@@ -164,6 +165,10 @@ struct sbwt_index {
     // bumped whenever a device structure a search reads is rebuilt (graph keys)
     uint64_t gen = 1;
     bool use_graph = false;
+    // L2 set-aside for the rank lines (l2_window): bytes this index asked for
+    // (0: none), and the device's limits
+    size_t l2_setaside = 0;
+    size_t l2_max_persist = 0, l2_max_window = 0;
     // per-call profiling (sbwt_profile_enable)
     bool prof_on = false;
     cudaEvent_t prof_ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -218,6 +223,13 @@ int search_rows_device(sbwt_index *ix, Workspace &w, const uint8_t *d_letters, u
                        u64 n_rows, u64 *d_answers, uint32_t *d_member, u64 n_kmers, cudaStream_t s);
 template <class T> int grow(T *&p, size_t &cap, size_t need);
 template <class T> int grow_host(T *&p, size_t &cap, size_t need);
+
+// api.cu: the L2 access-policy window of a search launch over the index's
+// current layout (false: none applies); l2_setaside_acquire/release size the
+// device's persisting set-aside for the indexes that use it.
+bool l2_window(const sbwt_index *ix, cudaAccessPolicyWindow *w);
+int l2_setaside_acquire(sbwt_index *ix);
+void l2_setaside_release(sbwt_index *ix);
 
 // search.cu
 int launch_search(const sbwt_index *ix, SearchArgs &a, cudaStream_t s, uint32_t *launched_blocks);

@@ -372,13 +372,15 @@ constexpr u32 kWin = 128;
 // lowest k-mer is settled; sectors that a long absent stretch covers whole
 // go out directly.  Only the sectors at the two ends of a run (row ends)
 // are stored answer by answer.  The stores carry the streaming (evict-first)
-// hint, so the answer stream does not push the index out of L2.  (The
-// previous form wrote ~0 over a warp's 32 windows when it took them and
-// overwrote the found answers later; the prefilled sectors had left L2 by
-// then, so each overwrite cost a DRAM read and a rewrite.)  Build option
-// SBWT_ANSWER_WRITE_ONCE=0 restores that form.
+// hint.  Build option SBWT_ANSWER_WRITE_ONCE=1.  The default form instead
+// writes ~0 over a warp's 32 windows when it takes them (coalesced, 256
+// bytes a store instruction) and overwrites the found answers later.
+// Measured on the large workload (ncu, 60M k-mers, full index): the
+// write-once form writes 7.9 instead of 8.7 bytes per k-mer but reads 25.5
+// instead of 22.5 and runs 10.3 ms instead of 8.3 ms a launch (more
+// instructions per settled k-mer, one store instruction per sector).
 #ifndef SBWT_ANSWER_WRITE_ONCE
-#define SBWT_ANSWER_WRITE_ONCE 1
+#define SBWT_ANSWER_WRITE_ONCE 0
 #endif
 
 #if SBWT_ANSWER_WRITE_ONCE
@@ -673,6 +675,27 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
 
 // -------------------------------------------------------------- dispatch
 
+// Launches a search kernel with the L2 access-policy window of the index's
+// rank lines, where one applies (l2_window).
+template <class K, class R>
+int launch_kernel(K kern, u32 blocks, u32 threads, cudaStream_t s, const sbwt_index *ix, const R &rk,
+                  const SearchArgs &a) {
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cfg.numAttrs = 0;
+    if (l2_window(ix, &attr[0].val.accessPolicyWindow)) {
+        attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    }
+    SBWT_CHECK_CUDA(cudaLaunchKernelEx(&cfg, kern, rk, a));
+    return 0;
+}
+
 template <class R, int KPT, int TPK>
 int launch_one(const R &rk, SearchArgs &a, const sbwt_index *ix, cudaStream_t s, u32 tpb, u32 *blocks_out) {
     auto kern = search_kernel<R, KPT, TPK>;
@@ -682,8 +705,7 @@ int launch_one(const R &rk, SearchArgs &a, const sbwt_index *ix, cudaStream_t s,
     const u32 blocks = (u32)per_sm * (u32)ix->num_sms;
     if (blocks_out) *blocks_out = blocks;
     SBWT_CHECK_CUDA(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), s));
-    kern<<<blocks, tpb, 0, s>>>(rk, a);
-    SBWT_CHECK_CUDA(cudaGetLastError());
+    SBWT_TRY(launch_kernel(kern, blocks, tpb, s, ix, rk, a));
     return 0;
 }
 
@@ -720,8 +742,7 @@ int launch_queue(const R &rk, SearchArgs &a, const sbwt_index *ix, cudaStream_t 
     const u32 blocks = (u32)per_sm * (u32)ix->num_sms;
     if (blocks_out) *blocks_out = blocks;
     SBWT_CHECK_CUDA(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), s));
-    kern<<<blocks, 128, 0, s>>>(rk, a);
-    SBWT_CHECK_CUDA(cudaGetLastError());
+    SBWT_TRY(launch_kernel(kern, blocks, 128u, s, ix, rk, a));
     return 0;
 }
 
