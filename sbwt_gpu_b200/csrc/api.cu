@@ -175,7 +175,7 @@ int finish_index(sbwt_index *ix, const u64 *const words[4], const sbwt_params *p
     for (int i = 0; i < 4; i++) SBWT_CHECK_CUDA(cudaEventElapsedTime(&ix->build_ms[i], ev[i], ev[i + 1]));
     if (!want_poppy) ix->build_ms[1] = 0.0f;
     if (!ix->stream_ok) ix->build_ms[3] = 0.0f;
-    return sbwt::l2_setaside_acquire(ix);
+    return 0;
 }
 
 int new_index(const sbwt_params *prm, sbwt_index **out, sbwt_index **ix_out) {
@@ -442,17 +442,16 @@ extern "C" int sbwt_set_search_mode(sbwt_index *ix, int32_t mode) {
 
 namespace sbwt {
 
-// The rank lines of the line layouts are the run walk's most reused data
-// (every rank-pair step reads one or two of them), but the answer stream and
-// the gathers from the presearch and backward tables (each larger than L2 on
-// the large workload) push them out: measured, the L2 hit rate of the walk
-// was 20-27 % and its DRAM reads 22-25 bytes per k-mer against 4.5 bytes of
-// gathers the tables need.  So the search launch carries an access-policy
-// window over the current layout's lines with the persisting property, and
-// the index sizes the device's persisting L2 set-aside to hold them (a CUDA
-// context limit, released again when the last index that asked for it is
-// freed).  Layouts larger than the set-aside (poppy, or lines beyond it) get
-// no window.
+// Option (KernelShape.l2_persist, environment SBWT_L2_PERSIST=1, tried by
+// the autotuner): the search launch carries an access-policy window over the
+// current layout's rank lines with the persisting property, and the index
+// sizes the device's persisting L2 set-aside to hold them (a CUDA context
+// limit, taken on the first such launch and released when the last index
+// that took it is freed).  Layouts larger than the set-aside (poppy, or lines
+// beyond it) get no window.  Measured on the large workload: 8.64 ms a
+// launch against 8.33 ms without (the lines are not what misses L2; the L2
+// hit rate stays at 20 %), and 11.4 ms with the set-aside carved out of L2
+// but no window, so it is off by default.
 namespace {
 std::mutex g_l2_mutex;
 constexpr int kL2Devices = 64;
@@ -461,7 +460,9 @@ size_t g_l2_set[kL2Devices] = {0};  // its size: the largest any of them asked f
 }  // namespace
 
 bool l2_window(const sbwt_index *ix, cudaAccessPolicyWindow *w) {
-    if (!ix->shape.l2_persist || ix->l2_setaside == 0) return false;
+    if (!ix->shape.l2_persist) return false;
+    if (ix->l2_setaside == 0) l2_setaside_acquire(const_cast<sbwt_index *>(ix));  // first windowed launch
+    if (ix->l2_setaside == 0) return false;
     const void *base = nullptr;
     size_t bytes = 0;
     if (ix->shape.layout == SBWT_LAYOUT_LINES && ix->lines_ok) {

@@ -15,8 +15,9 @@
 //   2. the run walk's knobs on the best layout, one at a time, each kept
 //      when it is faster: window (64 / 256 k-mers against 128), resident
 //      blocks per SM, the evict-first policy of the presearch and
-//      backward-table gathers (never / always against by table size), and
-//      the compact 4-byte presearch entries;
+//      backward-table gathers (never / always against by table size), the
+//      rank lines held in the persisting L2 set-aside, and the compact
+//      4-byte presearch entries;
 //   3. with SBWT_TUNE_P the presearch depth p in {8,10,12,14,15} (p <= k),
 //      then the window and the evict policy again at the chosen p.
 // Every candidate's answers are reduced to an order-sensitive checksum, and
@@ -48,7 +49,7 @@ struct Cand {
     int shuffles;
     u32 p;
     u32 window, bps;
-    int evict, compact;
+    int evict, compact, persist;
     float ms;
     unsigned long long sum;
 };
@@ -63,9 +64,9 @@ std::string cand_json(const Cand &c) {
     std::snprintf(b, sizeof b,
                   "{\"layout\":\"%s\",\"kmers_per_thread\":%u,\"threads_per_kmer\":%u,\"threads_per_block\":%u,"
                   "\"bits_in_superblock\":%u,\"shuffles\":%d,\"p\":%u,\"window\":%u,\"blocks_per_sm\":%u,"
-                  "\"evict\":\"%s\",\"compact_presearch\":%d,\"ms\":%.4f}",
+                  "\"evict\":\"%s\",\"compact_presearch\":%d,\"l2_persist\":%d,\"ms\":%.4f}",
                   layout_name(c.layout), c.kpt, c.tpk, c.tpb, c.sb, c.shuffles, c.p, c.window, c.bps,
-                  c.evict == 0 ? "by table size" : c.evict == 1 ? "never" : "always", c.compact, c.ms);
+                  c.evict == 0 ? "by table size" : c.evict == 1 ? "never" : "always", c.compact, c.persist, c.ms);
     return b;
 }
 
@@ -112,6 +113,8 @@ extern "C" int sbwt_autotune(sbwt_index *ix, const uint8_t *d_letters, uint64_t 
         ix->shape.window = c.window;
         ix->shape.blocks_per_sm = c.bps;
         ix->shape.evict = c.evict;
+        ix->shape.l2_persist = c.persist;
+        if (!c.persist && ix->l2_setaside) l2_setaside_release(ix);  // a set-aside without the window costs L2
         if (c.p != ix->p || c.compact != ix->compact_pre) {
             ix->compact_pre = c.compact;
             SBWT_TRY(run_presearch(ix, c.p, s));
@@ -161,16 +164,16 @@ extern "C" int sbwt_autotune(sbwt_index *ix, const uint8_t *d_letters, uint64_t 
         // stage 1: layouts; the first candidate is the index's configuration before tuning
         std::vector<Cand> stage1;
         stage1.push_back(Cand{saved.layout, saved.kpt, saved.tpk, saved.tpb, saved.sb, saved.shuffles, p0,
-                              saved.window, saved.blocks_per_sm, saved.evict, c0, 0, 0});
+                              saved.window, saved.blocks_per_sm, saved.evict, c0, saved.l2_persist, 0, 0});
         if (ix->lines_ok) {
             for (int l : {SBWT_LAYOUT_LINES, SBWT_LAYOUT_LINES512, SBWT_LAYOUT_LINES2048})
                 if (!(l == saved.layout && saved.kpt == 0 && saved.tpk == 1))
-                    stage1.push_back(Cand{l, 0, 1, 128, 1024, 0, p0, 128, 0, 0, c0, 0, 0});
+                    stage1.push_back(Cand{l, 0, 1, 128, 1024, 0, p0, 128, 0, 0, c0, 0, 0, 0});
             if (flags & 8u)
                 for (u32 tpb : {128u, 256u})
                     for (u32 tpk : {1u, 2u, 4u})
                         for (u32 kpt : {1u, 2u, 3u, 4u, 6u, 8u})
-                            stage1.push_back(Cand{SBWT_LAYOUT_LINES, kpt, tpk, tpb, 1024, 0, p0, 128, 0, 0, c0, 0, 0});
+                            stage1.push_back(Cand{SBWT_LAYOUT_LINES, kpt, tpk, tpb, 1024, 0, p0, 128, 0, 0, c0, 0, 0, 0});
         }
         if ((flags & 4u) || !ix->lines_ok)
             for (u32 sb : {512u, 1024u, 2048u})
@@ -180,7 +183,7 @@ extern "C" int sbwt_autotune(sbwt_index *ix, const uint8_t *d_letters, uint64_t 
                         if (kpt == 0 && sh) continue;
                         if (kpt && !(flags & 8u)) continue;
                         stage1.push_back(Cand{SBWT_LAYOUT_POPPY, kpt, 1, kpt == 0 ? 128u : 256u, sb, sh, p0, 128, 0, 0,
-                                              c0, 0, 0});
+                                              c0, 0, 0, 0});
                     }
                 }
         for (Cand &c : stage1)
@@ -213,6 +216,11 @@ extern "C" int sbwt_autotune(sbwt_index *ix, const uint8_t *d_letters, uint64_t 
                     c.bps = b;
                     SBWT_TRY(try_knob(c));
                 }
+            if (best.layout != SBWT_LAYOUT_POPPY) {  // the rank lines in the L2 set-aside
+                Cand c = best;
+                c.persist = best.persist ? 0 : 1;
+                SBWT_TRY(try_knob(c));
+            }
             if (compact && ix->n < dev::kPreMaxColumns && best.p) {
                 Cand c = best;
                 c.compact = best.compact == 1 ? 0 : 1;

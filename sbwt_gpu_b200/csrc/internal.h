@@ -74,7 +74,7 @@ struct KernelShape {
     u32 window = 128;        // k-mers per window (line layout: 64, 128 or 256)
     u32 blocks_per_sm = 0;   // resident blocks per SM of the persistent grid (0: as many as fit)
     int evict = 0;           // evict-first gathers: 0 = when a table exceeds half of L2, 1 = never, 2 = always
-    int l2_persist = 1;      // the rank lines of the search layout held in the L2 set-aside (l2_window)
+    int l2_persist = 0;      // the rank lines of the search layout held in the L2 set-aside (l2_window)
 };
 
 // Device buffers of one in-flight search (grow-only).
