@@ -63,6 +63,10 @@ def parse():
     ap.add_argument("--sb", type=int, default=1024, help="bits in superblock of the poppy layout")
     ap.add_argument("--l2-fetch", type=int, default=0, choices=[0, 32, 64, 128],
                     help="L2 fetch granularity in bytes for the searches (0: leave the device default)")
+    ap.add_argument("--window", type=int, default=0, choices=[0, 64, 128, 256], help="run-walk window (0: default)")
+    ap.add_argument("--evict", type=int, default=-1, choices=[-1, 0, 1, 2],
+                    help="evict-first gathers: 0 by table size, 1 never, 2 always (-1: default)")
+    ap.add_argument("--l2-persist", type=int, default=-1, choices=[-1, 0, 1], help="rank lines in the L2 set-aside")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-e2e", action="store_true")
@@ -549,6 +553,9 @@ def main():
               else ("search_queue_kernel" if args.kpt == 0 else "search_kernel"))
     if args.l2_fetch:
         ix.set_l2_fetch_granularity(args.l2_fetch)
+    if args.window or args.evict >= 0 or args.l2_persist >= 0:
+        ix.set_walk_options(window=args.window or None, evict=args.evict if args.evict >= 0 else None,
+                            l2_persist=args.l2_persist if args.l2_persist >= 0 else None)
     build_times = ix.build_times()  # device ms: rank words (lines), poppy, presearch, backward table
     info = ix.info()
 
@@ -837,9 +844,21 @@ def filtered_leg(ix, pf, sg, letters, rows, k, steps, dev, stream, plain_value, 
         raise SystemExit(f"bench: {label}: prefiltered answers differ (false-absent {false_absent})")
     value = n_kmers / (ms / 1e3)
     negatives = int((d_plain == -1).sum().item())
-    del d_letters, d_rows, d_ans, d_plain
+    # the model alone on the first 4M letters' k-mers: the share it rejects among absent and present ones
+    import oracle as orc
+    ns = int(np.searchsorted(rows, min(int(rows[-1]), 4_000_000)))
+    sk = orc.extract_kmers(letters[: int(rows[ns])], rows[: ns + 1], k)
+    d_sk = torch.from_numpy(sk.view(np.int64)).to(dev)
+    d_lg = torch.empty(d_sk.numel(), dtype=torch.float32, device=dev)
+    pf.logits(d_sk, d_lg)
+    absent = (d_plain[: d_sk.numel()] == -1)
+    rej = d_lg < 0.0  # the default threshold tau = 0 the prefilters here are trained with
+    model_reject_absent = float((rej & absent).sum().item()) / max(int(absent.sum().item()), 1)
+    model_reject_present = float((rej & ~absent).sum().item()) / max(int((~absent).sum().item()), 1)
+    del d_letters, d_rows, d_ans, d_plain, d_sk, d_lg
     torch.cuda.empty_cache()
     return {"workload": label, "plain_kmers_per_s": plain_value, "prefiltered_kmers_per_s": value,
+            "model_reject_rate_absent": model_reject_absent, "model_reject_rate_present": model_reject_present,
             "speedup": value / plain_value, "target_speedup": 1.5, "ms_per_call": ms, "skip_rate": skipped / n_kmers,
             "negative_fraction": negatives / n_kmers, "false_absent": false_absent, "bit_exact": equal,
             "entry_point": "sbwt_search_reads_filtered", "n_kmers": n_kmers, "stats": pf.stats()}

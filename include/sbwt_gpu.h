@@ -152,6 +152,17 @@ int sbwt_configure(sbwt_index *index, int32_t layout, uint32_t bits_in_superbloc
                    int32_t with_shuffles, uint32_t kmers_per_thread, uint32_t threads_per_kmer,
                    uint32_t threads_per_block);
 
+/* Knobs of the run walk (searches of reads), each SBWT_KEEP to leave it:
+ * window = k-mers per window of the work split (64, 128, 256; line layout),
+ * blocks_per_sm = resident blocks per SM of the persistent grid (0: as many
+ * as fit), evict = the L2 policy of the presearch and backward-table gathers
+ * (0: evict-first when the table exceeds half of L2, 1: never, 2: always),
+ * l2_persist = hold the rank lines in the persisting L2 set-aside (1) or not
+ * (0).  The autotuner sets them; the answers do not depend on them.  No
+ * reference counterpart. */
+int sbwt_set_walk_options(sbwt_index *index, uint32_t window, uint32_t blocks_per_sm, int32_t evict,
+                          int32_t l2_persist);
+
 /* Selects the search mode (SBWT_SEARCH_*) for later searches of reads on this
  * index, building the backward-step structures on first use of
  * SBWT_SEARCH_STREAM.  No reference counterpart: the reference searches every

@@ -151,6 +151,15 @@ class Index:
         check(lib.sbwt_build_times(self._h, ms))
         return {"lines_ms": ms[0], "poppy_ms": ms[1], "presearch_ms": ms[2], "backward_ms": ms[3]}
 
+    def set_walk_options(self, window=None, blocks_per_sm=None, evict=None, l2_persist=None):
+        """Knobs of the run walk (None: unchanged): window 64/128/256, resident blocks per SM (0: as many
+        as fit), evict 0 (by table size) / 1 (never) / 2 (always), l2_persist 0/1."""
+        keep = 0xFFFFFFFF
+        check(lib.sbwt_set_walk_options(self._h, keep if window is None else int(window),
+                                        keep if blocks_per_sm is None else int(blocks_per_sm),
+                                        -1 if evict is None else int(evict),
+                                        -1 if l2_persist is None else int(l2_persist)))
+
     def set_host_threads(self, threads):
         """Host threads of the host pipelines (0: the OpenMP default)."""
         check(lib.sbwt_set_host_threads(self._h, int(threads)))

@@ -151,6 +151,7 @@ SIGNATURES = {
     "sbwt_search_reads_host_multi": (c_int, [c_void_p, c_int, c_void_p, c_uint64, c_void_p, c_uint64, c_void_p,
                                              c_uint64]),
     "sbwt_partition_rows": (c_int, [c_void_p, c_uint64, c_uint32, c_int, c_void_p]),
+    "sbwt_set_walk_options": (c_int, [c_void_p, c_uint32, c_uint32, c_int32, c_int32]),
     "sbwt_set_host_threads": (c_int, [c_void_p, c_int]),
     "sbwt_pipeline_dense_share": (ctypes.c_double, [c_uint64, c_int]),
     "sbwt_search_reads_filtered": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_void_p, c_uint64, c_void_p,

@@ -429,6 +429,26 @@ extern "C" int sbwt_configure(sbwt_index *ix, int32_t layout, uint32_t sb, int32
     return 0;
 }
 
+extern "C" int sbwt_set_walk_options(sbwt_index *ix, uint32_t window, uint32_t blocks_per_sm, int32_t evict,
+                                     int32_t l2_persist) {
+    clear_error();
+    if (!ix) return set_error("index is NULL");
+    if (window != SBWT_KEEP && !(window == 64 || window == 128 || window == 256))
+        return set_error("window must be 64, 128 or 256 k-mers");
+    if (evict != (int32_t)SBWT_KEEP && (evict < 0 || evict > 2)) return set_error("evict must be 0, 1 or 2");
+    SBWT_CHECK_CUDA(cudaSetDevice(ix->device));
+    KernelShape &sh = ix->shape;
+    if (window != SBWT_KEEP) sh.window = window;
+    if (blocks_per_sm != SBWT_KEEP) sh.blocks_per_sm = blocks_per_sm;
+    if (evict != (int32_t)SBWT_KEEP) sh.evict = evict;
+    if (l2_persist != (int32_t)SBWT_KEEP) {
+        sh.l2_persist = l2_persist != 0;
+        if (!sh.l2_persist && ix->l2_setaside) l2_setaside_release(ix);
+    }
+    ix->gen++;
+    return 0;
+}
+
 extern "C" int sbwt_set_search_mode(sbwt_index *ix, int32_t mode) {
     clear_error();
     if (!ix) return set_error("index is NULL");

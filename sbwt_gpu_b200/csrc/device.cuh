@@ -38,17 +38,35 @@ constexpr u32 kMaxLinesPerChar = 1u << 24;  // 32-bit counts: 224 * 2^24 < 2^32
 #define SBWT_LINES_EVICT_LAST 0
 #endif
 
+// Cache operator of the random gathers: SBWT_GATHER_CG = 1 reads the
+// presearch and backward-table entries with ld.global.cg (cached in L2
+// only), 2 also the rank lines; 0 reads them through the read-only L1 path
+// (ld.global.nc).
+#ifndef SBWT_GATHER_CG
+#define SBWT_GATHER_CG 0
+#endif
+#if SBWT_GATHER_CG >= 2
+#define SBWT_LINE_LD "ld.global.cg"
+#else
+#define SBWT_LINE_LD "ld.global.nc"
+#endif
+#if SBWT_GATHER_CG >= 1
+#define SBWT_GATHER_LD "ld.global.cg"
+#else
+#define SBWT_GATHER_LD "ld.global.nc"
+#endif
+
 // 256-bit read-only load of one line (sm_100 supports .v4.u64 global loads).
 __device__ __forceinline__ ulonglong4 ld_line(const ulonglong4 *p) {
     ulonglong4 v;
 #if SBWT_LINES_EVICT_LAST
     u64 pol;
     asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
-    asm("ld.global.nc.L2::cache_hint.v4.u64 {%0, %1, %2, %3}, [%4], %5;"
+    asm(SBWT_LINE_LD ".L2::cache_hint.v4.u64 {%0, %1, %2, %3}, [%4], %5;"
         : "=l"(v.x), "=l"(v.y), "=l"(v.z), "=l"(v.w)
         : "l"(p), "l"(pol));
 #else
-    asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];"
+    asm(SBWT_LINE_LD ".v4.u64 {%0, %1, %2, %3}, [%4];"
         : "=l"(v.x), "=l"(v.y), "=l"(v.z), "=l"(v.w)
         : "l"(p));
 #endif
@@ -103,7 +121,7 @@ __device__ __forceinline__ uint2 ld_gather_u32x2(const uint2 *p, bool ef, u64 po
 #if SBWT_GATHER_EVICT_FIRST
     if (ef) {
         uint2 v;
-        asm("ld.global.nc.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;" : "=r"(v.x), "=r"(v.y) : "l"(p), "l"(pol));
+        asm(SBWT_GATHER_LD ".L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;" : "=r"(v.x), "=r"(v.y) : "l"(p), "l"(pol));
         return v;
     }
 #endif
@@ -116,7 +134,7 @@ __device__ __forceinline__ u64 ld_gather_u64(const u64 *p, bool ef, u64 pol) {
 #if SBWT_GATHER_EVICT_FIRST
     if (ef) {
         u64 v;
-        asm("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(p), "l"(pol));
+        asm(SBWT_GATHER_LD ".L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(p), "l"(pol));
         return v;
     }
 #endif
