@@ -767,7 +767,7 @@ def autotune_leg(ix, letters, rows, d_ans, n_kmers, k, step, ans, steps, dev, st
     """The tuner picks the run walk's knobs and the presearch depth on a sample, then the batch is timed again."""
     import torch
     import sbwt_gpu_b200 as sg
-    ns = min(rows.size - 1, 1_000_000)
+    ns = min(rows.size - 1, 3_000_000)  # 360M k-mers of the large batch: choices that carry over to the whole batch
     nk_s = sg.count_kmers(rows[: ns + 1], k)
     d_ls = torch.from_numpy(letters[: int(rows[ns])]).to(dev)
     d_rs = torch.from_numpy(rows[: ns + 1].view(np.int64)).to(dev)
