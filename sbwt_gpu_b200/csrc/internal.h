@@ -155,9 +155,9 @@ struct sbwt_index {
     size_t scan_cap = 0;
     // per-call work buffers: ws[0] serves the device-pointer entry points,
     // ws[0 .. kPipeSlots) the streams of the host pipeline
-    static constexpr int kPipeSlots = 4;
+    static constexpr int kPipeSlots = 6;
     sbwt::Workspace ws[kPipeSlots];
-    cudaStream_t pipe_stream[kPipeSlots] = {nullptr, nullptr, nullptr, nullptr};
+    cudaStream_t pipe_stream[kPipeSlots] = {};
     // bytes the last host-pipeline call copied host->device and device->host
     uint64_t pipe_h2d = 0, pipe_d2h = 0;
     // host threads of the host pipelines (0: the OpenMP default)

@@ -124,8 +124,8 @@ __device__ __forceinline__ void onehot_chunks(uint8_t *tile, u32 R, u32 r, u64 k
 }
 
 // One CTA per SM (226 KiB of shared memory, all 512 TMEM columns), 512
-// threads = 16 warps.  b1, b2 and w3 must be 16-byte aligned (float4 loads;
-// their offsets in the parameter vector are multiples of 4 floats).  Warp w
+// threads = 16 warps.  The biases and w3 come by value in the parameter
+// space (InferBias, read as float4 through the constant cache).  Warp w
 // reaches TMEM lanes 32*(w%4)..+31 (rows of the 128-k-mer tile) and handles
 // hidden columns 64*(w/4)..+63 of them in both epilogues, so four warps
 // share each row and the epilogues run on all 16 warps; layer 2's 256 -> 1
@@ -140,7 +140,7 @@ __device__ __forceinline__ void onehot_chunks(uint8_t *tile, u32 R, u32 r, u64 k
 // tile t's layer-2 MMA runs:
 //   epi1(t) -> MMA2(t) || one-hot(t+1) -> MMA1(t+1) || epi2(t) -> epi1(t+1) ...
 // Two mbarriers (layer 1, layer 2), each with its own phase.
-__device__ __forceinline__ void infer_epi1(u32 tacc, u32 ta2, u32 lane_base, u32 c0, const float *__restrict__ b1) {
+__device__ __forceinline__ void infer_epi1(u32 tacc, u32 ta2, u32 lane_base, u32 c0, const InferBias &bias) {
     u32 v[4][16];
 #pragma unroll
     for (u32 j = 0; j < 4; j++) tmem_ld16(tacc + lane_base + c0 + 16u * j, v[j]);
@@ -151,8 +151,8 @@ __device__ __forceinline__ void infer_epi1(u32 tacc, u32 ta2, u32 lane_base, u32
         u32 packed[8];
 #pragma unroll
         for (int t = 0; t < 16; t += 4) {
-            // the same 4 biases for every lane of the warp: one 16-byte load
-            const float4 bb = __ldg(reinterpret_cast<const float4 *>(b1 + c0 + 16u * j + t));
+            // the same 4 biases for every lane of the warp, from the parameter space
+            const float4 bb = *reinterpret_cast<const float4 *>(bias.b1 + c0 + 16u * j + t);
             packed[t / 2] = pack_bf16x2(fmaxf(__uint_as_float(v[j][t]) + bb.x, 0.0f),
                                         fmaxf(__uint_as_float(v[j][t + 1]) + bb.y, 0.0f));
             packed[t / 2 + 1] = pack_bf16x2(fmaxf(__uint_as_float(v[j][t + 2]) + bb.z, 0.0f),
@@ -164,8 +164,7 @@ __device__ __forceinline__ void infer_epi1(u32 tacc, u32 ta2, u32 lane_base, u32
 }
 
 // Partial dot of one row's 64 layer-2 activations (bias, ReLU, BF16) with w3.
-__device__ __forceinline__ float infer_epi2(u32 tacc, u32 lane_base, u32 c0, const float *__restrict__ b2,
-                                            const float *__restrict__ w3) {
+__device__ __forceinline__ float infer_epi2(u32 tacc, u32 lane_base, u32 c0, const InferBias &bias) {
     u32 v[4][16];
 #pragma unroll
     for (u32 j = 0; j < 4; j++) tmem_ld16(tacc + lane_base + c0 + 16u * j, v[j]);
@@ -177,8 +176,8 @@ __device__ __forceinline__ float infer_epi2(u32 tacc, u32 lane_base, u32 c0, con
 #pragma unroll
         for (int t = 0; t < 16; t += 4) {
             const u32 c = c0 + 16u * j + t;
-            const float4 bb = __ldg(reinterpret_cast<const float4 *>(b2 + c));
-            const float4 ww = __ldg(reinterpret_cast<const float4 *>(w3 + c));
+            const float4 bb = *reinterpret_cast<const float4 *>(bias.b2 + c);
+            const float4 ww = *reinterpret_cast<const float4 *>(bias.w3 + c);
             acc = fmaf(bf16_round(fmaxf(__uint_as_float(v[j][t]) + bb.x, 0.0f)), ww.x, acc);
             acc = fmaf(bf16_round(fmaxf(__uint_as_float(v[j][t + 1]) + bb.y, 0.0f)), ww.y, acc);
             acc = fmaf(bf16_round(fmaxf(__uint_as_float(v[j][t + 2]) + bb.z, 0.0f)), ww.z, acc);
@@ -190,8 +189,7 @@ __device__ __forceinline__ float infer_epi2(u32 tacc, u32 lane_base, u32 c0, con
 
 __global__ void __launch_bounds__(kInferThreads, 1)
     mlp_infer_kernel(const u64 *__restrict__ kmers, u64 n, u32 k, const bf16 *__restrict__ W1b,
-                     const bf16 *__restrict__ W2b, const float *__restrict__ b1, const float *__restrict__ b2,
-                     const float *__restrict__ w3, const float *__restrict__ b3, const InferOut out, int *err) {
+                     const bf16 *__restrict__ W2b, const InferBias bias, const InferOut out, int *err) {
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ uint64_t bar1, bar2;
     __shared__ u32 tmem_s;
@@ -233,7 +231,7 @@ __global__ void __launch_bounds__(kInferThreads, 1)
     fence_after_sync();
     const u32 T0 = tmem_s;
     const u32 lane_base = (quarter * 32u) << 16;
-    const float bias3 = __ldg(b3);
+    const float bias3 = bias.b3;
     auto mma1 = [&](u32 tacc) {  // layer 1: one-hot tile x W1^T into tacc (thread 0, after a thread sync)
         fence_after_sync();
 #pragma unroll
@@ -258,7 +256,7 @@ __global__ void __launch_bounds__(kInferThreads, 1)
         pend1 = false;
         fence_after_sync();
         if (!__syncthreads_and(got)) { ok = false; break; }
-        infer_epi1(tacc, ta2, lane_base, c0, b1);
+        infer_epi1(tacc, ta2, lane_base, c0, bias);
         fence_before_sync();
         __syncthreads();
         if (tid == 0) {
@@ -290,7 +288,7 @@ __global__ void __launch_bounds__(kInferThreads, 1)
             pend1 = true;
         }
         // ---- this tile's layer-2 epilogue while the next tile's layer 1 runs
-        sRed[cg * kTileM + trow] = infer_epi2(tacc, lane_base, c0, b2, w3);
+        sRed[cg * kTileM + trow] = infer_epi2(tacc, lane_base, c0, bias);
         fence_before_sync();
         __syncthreads();
         if (cg == 0) {
@@ -624,7 +622,7 @@ int gemm_tn(const bf16 *A, const bf16 *B, float *D, u32 M, u32 N, u32 K, u32 spl
     return 0;
 }
 
-int infer(const u64 *kmers, u64 n, u32 k, const bf16 *W1b, const bf16 *W2b, const float *theta, const MlpOffsets &off,
+int infer(const u64 *kmers, u64 n, u32 k, const bf16 *W1b, const bf16 *W2b, const InferBias &bias,
           const InferOut &out, int *err, int num_sms, cudaStream_t s) {
     if (n == 0) return 0;
     // the shared-memory opt-in is a per-device function attribute
@@ -636,12 +634,9 @@ int infer(const u64 *kmers, u64 n, u32 k, const bf16 *W1b, const bf16 *W2b, cons
         SBWT_CHECK_CUDA(cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem));
         attr_set[dev] = true;
     }
-    for (const float *q : {theta + off.b1, theta + off.b2, theta + off.w3})
-        if ((uintptr_t)q & 15u) return set_error("MLP parameters must be 16-byte aligned");
     const u64 tiles = (n + kTileM - 1) / kTileM;
     const u32 grid = (u32)std::min<u64>(tiles, (u64)num_sms);
-    mlp_infer_kernel<<<grid, kInferThreads, kInferSmem, s>>>(kmers, n, k, W1b, W2b, theta + off.b1, theta + off.b2,
-                                                   theta + off.w3, theta + off.b3, out, err);
+    mlp_infer_kernel<<<grid, kInferThreads, kInferSmem, s>>>(kmers, n, k, W1b, W2b, bias, out, err);
     SBWT_CHECK_CUDA(cudaGetLastError());
     return 0;
 }

@@ -64,8 +64,26 @@ struct InferOut {
 constexpr int kMaxDevicesAttr = 64;
 inline InferOut logits_only(float *logits) { return InferOut{logits, nullptr, 0.0f, nullptr, 0, 0}; }
 
+// The biases and the output weights of an inference launch, passed by value:
+// they are the same for every thread of a warp, so in the parameter space
+// they are read through the constant cache instead of the global-load queue.
+struct alignas(16) InferBias {  // 16-byte aligned: the epilogues read it as float4
+    float b1[256];
+    float b2[256];
+    float w3[256];
+    float b3;
+};
+inline void bias_from_host(const float *theta, const MlpOffsets &off, InferBias &b) {
+    for (int i = 0; i < 256; i++) {
+        b.b1[i] = theta[off.b1 + i];
+        b.b2[i] = theta[off.b2 + i];
+        b.w3[i] = theta[off.w3 + i];
+    }
+    b.b3 = theta[off.b3];
+}
+
 int infer(const uint64_t *kmers, uint64_t n, uint32_t k, const __nv_bfloat16 *W1b, const __nv_bfloat16 *W2b,
-          const float *theta, const MlpOffsets &off, const InferOut &out, int *err, int num_sms, cudaStream_t s);
+          const InferBias &bias, const InferOut &out, int *err, int num_sms, cudaStream_t s);
 int transpose(const __nv_bfloat16 *src, __nv_bfloat16 *dst, uint32_t R, uint32_t C, cudaStream_t s);
 
 }  // namespace mlp

@@ -1,19 +1,21 @@
 // pipeline.cu -- sbwt_search_reads_host: a batch of reads in host memory is
-// streamed through the GPU in chunks of rows.  Four CUDA streams take
-// turns; on each, a chunk's letters and row table go host->device, the chunk
-// is packed and searched, and its answers come back device->host, so the
+// streamed through the GPU in chunks of rows.  Six CUDA streams take turns;
+// on each, a chunk's letters and row table go host->device, the chunk is
+// packed and searched, and its answers come back device->host, so the
 // copies of one chunk overlap the search of another while the host prepares
 // the next.
 //
 // The u64 answers do not cross PCIe as such (8 bytes a k-mer would make the
-// device->host copy the bound): while node ids fit in 32 bits and at least
-// six host threads can expand them, a chunk comes back as its membership
-// bitmap, per-group offsets and the found node ids, and the host threads
-// expand them into the caller's answers.  Per chunk b the loop issues b,
-// starts the node-id copy of b-2 (its count is known once b-2's bitmap and
-// offsets are in) and expands b-3, so that two chunks keep the copy engines
-// and the GPU busy while the host threads expand.  Hybrid: every fourth
-// chunk's u64 answers go by DMA into the caller's pinned buffer instead.
+// device->host copy the bound): while node ids fit in 32 bits, a chunk comes
+// back as its membership bitmap, per-group offsets and the found node ids,
+// and host threads expand them into the caller's answers.  Per chunk b the
+// issuing thread issues b, starts the node-id copy of b-2 (its count is known
+// once b-2's bitmap and offsets are in) and hands b-3 to an expander thread,
+// which expands it with the other host threads while the issuing thread goes
+// on; a slot's buffers are reused (by chunk b+6) only once its expansion is
+// done.
+// With few host threads, a share of the chunks comes back as u64 answers by
+// DMA straight into the caller's pinned buffer instead (dense_share).
 //
 // This replaces the strictly sequential host<->device chain of the reference
 // (KmerSearch::search, include/epicseq/kmer_search.hpp:97-160: one H2D of the
@@ -21,7 +23,10 @@
 // ResultsPersister::save_results_to_file, results_persister.hpp:58-65).
 #include <algorithm>
 #include <cstdlib>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -280,6 +285,71 @@ using namespace sbwt;
 namespace sbwt {
 namespace {
 
+struct ExpandJob {
+    u64 *answers;
+    u64 nk;
+    const uint32_t *member;
+    const u64 *goff;
+    const uint32_t *nodes;
+};
+
+// One thread that expands the sparse answers of the chunks handed to it, in
+// order, with `threads` OpenMP threads.  Destroying it (also on an error
+// return of the pipeline) finishes the jobs already handed over.
+struct Expander {
+    std::thread th;
+    std::mutex m;
+    std::condition_variable cv;
+    std::deque<std::pair<int, ExpandJob>> jobs;
+    int busy[sbwt_index::kPipeSlots] = {};  // jobs queued or running per slot
+    bool stop = false, running = false;
+    int threads = 1;
+
+    void start(int t) {
+        threads = t;
+        running = true;
+        th = std::thread([this] {
+            for (;;) {
+                std::pair<int, ExpandJob> j;
+                {
+                    std::unique_lock<std::mutex> lk(m);
+                    cv.wait(lk, [this] { return stop || !jobs.empty(); });
+                    if (jobs.empty()) return;
+                    j = jobs.front();
+                    jobs.pop_front();
+                }
+                const ExpandJob &e = j.second;
+                expand_answers(e.answers, e.nk, e.member, e.goff, e.nodes, threads);
+                std::lock_guard<std::mutex> lk(m);
+                busy[j.first]--;
+                cv.notify_all();
+            }
+        });
+    }
+    void submit(int slot, const ExpandJob &e) {
+        std::lock_guard<std::mutex> lk(m);
+        jobs.emplace_back(slot, e);
+        busy[slot]++;
+        cv.notify_all();
+    }
+    void wait_slot(int slot) {
+        if (!running) return;
+        std::unique_lock<std::mutex> lk(m);
+        cv.wait(lk, [&] { return busy[slot] == 0; });
+    }
+    void finish() {
+        if (!running) return;
+        {
+            std::lock_guard<std::mutex> lk(m);
+            stop = true;
+            cv.notify_all();
+        }
+        th.join();
+        running = false;
+    }
+    ~Expander() { finish(); }
+};
+
 // The pipeline behind both host entry points: exactly one of `answers`
 // (u64 per k-mer) and `member` (bit j%32 of word j/32) is non-NULL.
 int pipeline_chunks(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, const uint64_t *row_starts,
@@ -402,6 +472,12 @@ int pipeline_chunks(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, 
         ix->pipe_d2h += found * sizeof(uint32_t);
         return 0;
     };
+    // Sparse chunks are expanded by an expander thread of their own (with the
+    // host threads but one), so that this thread keeps issuing chunks and
+    // waiting on their copies meanwhile; a slot is reused only once the
+    // expander is done with its host buffers.
+    Expander ex;
+    if (sparse) ex.start(threads > 1 ? threads - 1 : 1);
     auto drain = [&](int slot) -> int {
         SBWT_TRY(fetch_nodes(slot));
         SBWT_CHECK_CUDA(cudaStreamSynchronize(ix->pipe_stream[slot]));
@@ -410,7 +486,7 @@ int pipeline_chunks(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, 
             const Chunk &c = chunks[(size_t)pending[slot]];
             Workspace &w = ix->ws[slot];
             if (sparse) {
-                expand_answers(answers + c.k0, c.nk, w.h_member, w.h_goff, w.h_nodes, threads);
+                ex.submit(slot, ExpandJob{answers + c.k0, c.nk, w.h_member, w.h_goff, w.h_nodes});
             } else if (answers) {
                 std::memcpy(answers + c.k0, w.h_answers, c.nk * sizeof(u64));
             } else {
@@ -440,6 +516,7 @@ int pipeline_chunks(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, 
         cudaStream_t s = ix->pipe_stream[slot];
         Workspace &w = ix->ws[slot];
         SBWT_TRY(drain(slot));  // slot's previous chunk has finished with its buffers
+        ex.wait_slot(slot);     // and the expander with its host buffers
         const u64 nr = c.r1 - c.r0, nl = c.l1 - c.l0;
         uint64_t *hr = w.h_rows;
 #pragma omp parallel for schedule(static) if (nr > (1u << 16))
@@ -503,6 +580,7 @@ int pipeline_chunks(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, 
     }
     // the chunks still in flight, oldest first
     for (size_t i = 0; i < (size_t)kSlots; i++) SBWT_TRY(drain((int)((chunks.size() + i) % kSlots)));
+    ex.finish();
     return 0;
 }
 

@@ -48,6 +48,8 @@ struct sbwt_prefilter {
     size_t reject_cap = 0;
     uint64_t *d_klist = nullptr;
     size_t klist_cap = 0;
+    // host copy of the trained biases and output weights (inference parameters)
+    sbwt::mlp::InferBias bias{};
     sbwt_prefilter_stats stats{};
 };
 
@@ -329,12 +331,18 @@ extern "C" int sbwt_prefilter_train(sbwt_index *ix, const sbwt_mlp_params *prm, 
         SBWT_CHECK_CUDA(cudaMemcpyAsync(pf->theta, t.theta, t.off.count * sizeof(float), cudaMemcpyDeviceToDevice, s));
         SBWT_CHECK_CUDA(cudaMemcpyAsync(pf->W1b, t.W1b, 256 * 128 * sizeof(bf16), cudaMemcpyDeviceToDevice, s));
         SBWT_CHECK_CUDA(cudaMemcpyAsync(pf->W2b, t.W2b, 256 * 256 * sizeof(bf16), cudaMemcpyDeviceToDevice, s));
+        {
+            std::vector<float> th(t.off.count);
+            SBWT_CHECK_CUDA(cudaMemcpyAsync(th.data(), t.theta, t.off.count * sizeof(float), cudaMemcpyDeviceToHost, s));
+            SBWT_CHECK_CUDA(cudaStreamSynchronize(s));
+            bias_from_host(th.data(), t.off, pf->bias);
+        }
         // accuracy on the training candidates (first min(n, 4M)) at tau
         {
             const uint64_t na = std::min<uint64_t>(n_train, 4u << 20);
             float *lg = nullptr;
             SBWT_CHECK_CUDA(cudaMalloc(&lg, na * sizeof(float)));
-            rc = infer(d_train, na, ix->k, pf->W1b, pf->W2b, pf->theta, pf->off, logits_only(lg), pf->d_err, ix->num_sms, s);
+            rc = infer(d_train, na, ix->k, pf->W1b, pf->W2b, pf->bias, logits_only(lg), pf->d_err, ix->num_sms, s);
             if (rc == 0) {
                 accuracy_kernel<<<(unsigned)((na + 255) / 256), 256, 0, s>>>(lg, d_labels, na, pf->tau, d_cnt + 1);
                 unsigned long long cnt[2];
@@ -353,7 +361,7 @@ extern "C" int sbwt_prefilter_train(sbwt_index *ix, const sbwt_mlp_params *prm, 
         SBWT_CHECK_CUDA(cudaMalloc(&lg, nodes * sizeof(float)));
         enumerate_kernel<<<(unsigned)((nodes + 255) / 256), 256, 0, s>>>(ix->d_lines, ix->lpc, c5, (uint32_t)ix->n,
                                                                          ix->k, d_all);
-        rc = infer(d_all, nodes, ix->k, pf->W1b, pf->W2b, pf->theta, pf->off, logits_only(lg), pf->d_err, ix->num_sms, s);
+        rc = infer(d_all, nodes, ix->k, pf->W1b, pf->W2b, pf->bias, logits_only(lg), pf->d_err, ix->num_sms, s);
         if (rc == 0) {
             cudaMemsetAsync(d_cnt + 2, 0, sizeof(unsigned long long), s);
             bloom_build_kernel<<<(unsigned)((nodes + 255) / 256), 256, 0, s>>>(d_all, lg, nodes, pf->tau, ix->k,
@@ -454,7 +462,7 @@ extern "C" int sbwt_prefilter_logits(sbwt_prefilter *pf, const uint64_t *d_kmers
     SBWT_CHECK_CUDA(cudaSetDevice(pf->device));
     int dev_sms = 0;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, pf->device);
-    return infer(d_kmers, n, pf->k, pf->W1b, pf->W2b, pf->theta, pf->off, logits_only(d_logits), pf->d_err, dev_sms,
+    return infer(d_kmers, n, pf->k, pf->W1b, pf->W2b, pf->bias, logits_only(d_logits), pf->d_err, dev_sms,
                  (cudaStream_t)stream);
 }
 
@@ -486,7 +494,7 @@ extern "C" int sbwt_search_kmers_filtered(sbwt_index *ix, sbwt_prefilter *pf, co
         SBWT_CHECK_CUDA(cudaMalloc(&pf->d_logits, n * sizeof(float)));
         pf->logits_cap = n;
     }
-    SBWT_TRY(infer(d_kmers, n, pf->k, pf->W1b, pf->W2b, pf->theta, pf->off, logits_only(pf->d_logits), pf->d_err,
+    SBWT_TRY(infer(d_kmers, n, pf->k, pf->W1b, pf->W2b, pf->bias, logits_only(pf->d_logits), pf->d_err,
                    ix->num_sms, s));
     SBWT_CHECK_CUDA(cudaMemsetAsync(pf->d_skipped, 0, sizeof(unsigned long long), s));
     SBWT_TRY(search_list(ix, d_kmers, n, d_answers, pf->d_logits, pf, pf->d_skipped, s));
@@ -546,7 +554,7 @@ extern "C" int sbwt_search_reads_filtered(sbwt_index *ix, sbwt_prefilter *pf, co
         SBWT_TRY(launch_kmer_list(a, j0, cnt, pf->d_klist, s));
         InferOut o = out;
         o.reject = pf->d_reject + j0 / 32;
-        SBWT_TRY(infer(pf->d_klist, cnt, pf->k, pf->W1b, pf->W2b, pf->theta, pf->off, o, pf->d_err, ix->num_sms, s));
+        SBWT_TRY(infer(pf->d_klist, cnt, pf->k, pf->W1b, pf->W2b, pf->bias, o, pf->d_err, ix->num_sms, s));
     }
     SBWT_CHECK_CUDA(cudaMemsetAsync(pf->d_skipped, 0, sizeof(unsigned long long), s));
     a.reject = pf->d_reject;
@@ -619,7 +627,9 @@ extern "C" int sbwt_mlp_logits(uint32_t k, const float *theta, const uint64_t *k
         to_bf16_kernel<<<(256 * 256 + 255) / 256, 256>>>(d_th + off.W2, w2, 256 * 256);
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
-        rc = infer(d_k, n, k, w1, w2, d_th, off, logits_only(d_lg), err, sms, 0);
+        InferBias hb;
+        bias_from_host(theta, off, hb);
+        rc = infer(d_k, n, k, w1, w2, hb, logits_only(d_lg), err, sms, 0);
         if (rc == 0) {
             cudaError_t e = cudaDeviceSynchronize();
             if (e != cudaSuccess) rc = set_error("inference failed: %s", cudaGetErrorString(e));

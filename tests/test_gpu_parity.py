@@ -549,7 +549,7 @@ def test_host_pipelines_across_chunks(small, cuda):
 def test_host_answers_sparse_transfer_many_chunks(small, cuda, monkeypatch, chunk, transfer):
     """The host answers pipeline brings a chunk's answers back as its membership bitmap, group
     offsets and found node ids and expands them on the host (or, dense, as u64 answers).  Many
-    chunks (every stage of the four-slot rotation), chunks where every k-mer is found (genome
+    chunks (every stage of the six-slot rotation and of the expander thread), chunks where every k-mer is found (genome
     reads only), reads without a found k-mer, ragged, empty and shorter-than-k rows, against the
     oracle."""
     import torch
