@@ -201,6 +201,7 @@ int new_index(const sbwt_params *prm, sbwt_index **out, sbwt_index **ix_out) {
     ix->l2_max_persist = mp > 0 ? (size_t)mp : 0;
     ix->l2_max_window = mw > 0 ? (size_t)mw : 0;
     if (const char *e = std::getenv("SBWT_L2_PERSIST")) ix->shape.l2_persist = std::atoi(e) != 0;
+    if (const char *e = std::getenv("SBWT_RUN_INDEX64")) ix->shape.index64 = std::atoi(e) != 0;
     *ix_out = ix;
     return 0;
 }
@@ -559,6 +560,7 @@ SearchArgs base_args(const sbwt_index *ix, bool rows) {
     a.chunk = search_chunk(ix, rows);
     a.runs = rows && runs_form(ix);
     a.stream = a.runs && stream_form(ix);
+    a.index64 = (u32)ix->shape.index64;
     a.pre32 = a.runs ? ix->d_pre32 : nullptr;
     if (a.stream) a.sv = stream_view(ix);
     set_gather_policies(ix, a);

@@ -43,6 +43,7 @@ struct SearchArgs {
     u32 chunk;                    // k-mers per grab; with `runs`, k-mers per window of chunk_row
     u32 runs;                     // read mode: walk runs right to left with the absent-run skip
     u32 stream;                   // with `runs`: backward steps from a found k-mer (needs sv)
+    u32 index64;                  // with `runs`: the walk's 64-bit index form whatever the batch size
     u32 ef_pre, ef_back;          // with `runs`: evict-first gathers from the presearch / backward
                                   // table (each set when that table cannot stay in L2; device.cuh)
     dev::StreamView sv;           // backward table, node nibbles, select samples (stream.cuh)
@@ -75,6 +76,7 @@ struct KernelShape {
     u32 blocks_per_sm = 0;   // resident blocks per SM of the persistent grid (0: as many as fit)
     int evict = 0;           // evict-first gathers: 0 = when a table exceeds half of L2, 1 = never, 2 = always
     int l2_persist = 0;      // the rank lines of the search layout held in the L2 set-aside (l2_window)
+    int index64 = 0;         // 64-bit k-mer and letter indices even for batches that fit 32 bits
 };
 
 // Device buffers of one in-flight search (grow-only).

@@ -98,7 +98,8 @@ constexpr u32 kGroupWarps = 4;  // groups (warps) per block of group_nodes_kerne
 // evenly over the chunks (2 threads, as under torchrun with 8 ranks on 16
 // cores: 72 % dense, about 1.4x the all-dense time; 1 thread: 84 %).  The
 // environment variable SBWT_PIPELINE_TRANSFER = dense | sparse | hybrid
-// (every fourth chunk dense) overrides the choice.
+// (every fourth chunk dense) overrides the choice, and
+// SBWT_PIPELINE_DENSE_SHARE = f in [0, 1] sets the share itself.
 enum Transfer { kDense, kSparse, kSplit };
 constexpr int kMinExpandThreads = 6;
 constexpr double kExpandPerThread = 11e9;  // bytes of u64 answers per second per host thread (measured)
@@ -118,6 +119,9 @@ double dense_share(u64 n, int T, Transfer *mode) {
         t = kSparse, f = 0.0;
     } else if (e && std::strcmp(e, "hybrid") == 0) {
         t = kSplit, f = 0.25;
+    } else if (const char *d = std::getenv("SBWT_PIPELINE_DENSE_SHARE")) {
+        f = std::min(1.0, std::max(0.0, std::atof(d)));
+        t = f >= 1.0 ? kDense : f <= 0.0 ? kSparse : kSplit;
     } else if (T >= kMinExpandThreads) {
         t = kSparse, f = 0.0;
     } else {

@@ -446,11 +446,26 @@ __device__ __forceinline__ void stage_absent(u64 *ans, u64 *slot, u64 x, u64 b, 
 // (56 registers; 8 blocks at the compiler's 60 registers was 13 % slower),
 // 10 for the poppy ranker with basic blocks of up to 256 bits (48 registers);
 // the larger poppy blocks keep the compiler's choice (a cap spills there).
-template <class R> struct RunsMinBlocks { static constexpr int value = 1; };
-template <int TPK> struct RunsMinBlocks<LinesRankerT<TPK>> { static constexpr int value = 9; };
-template <int S> struct RunsMinBlocks<WideRanker<S>> { static constexpr int value = 8; };
-template <int SB, int KIND, class IT, int TPK> struct RunsMinBlocks<PoppyRanker<SB, KIND, IT, TPK>> {
-    static constexpr int value = SB <= 1024 ? 10 : 1;
+// The form with 32-bit k-mer and letter indices (IX = u32, batches below 4G
+// letters) needs 52-55 registers uncapped instead of 56 + 12 bytes of spill.
+// Measured on the large workload (p = 12 / 15): 9 blocks 8.25 / 7.32 ms
+// (the 64-bit form: 8.32 / 7.38), 10 blocks (48 registers, 20 bytes of
+// spill) 8.32 / 7.38, 12 blocks (40 registers, 82 bytes) 8.94 / 8.25.
+#ifndef SBWT_RUNS_BLOCKS32
+#define SBWT_RUNS_BLOCKS32 9
+#endif
+// The same for the poppy ranker with basic blocks of up to 512 bits (44-46
+// registers at 10 blocks, no spill): basic blocks of 512 bits, 10 blocks
+// 8.16 / 7.44 ms, 12 blocks 8.32 / 7.68.
+#ifndef SBWT_RUNS_BLOCKS32_POPPY
+#define SBWT_RUNS_BLOCKS32_POPPY 10
+#endif
+template <class R, class IX> struct RunsMinBlocks { static constexpr int value = 1; };
+template <int TPK> struct RunsMinBlocks<LinesRankerT<TPK>, u64> { static constexpr int value = 9; };
+template <int TPK> struct RunsMinBlocks<LinesRankerT<TPK>, u32> { static constexpr int value = SBWT_RUNS_BLOCKS32; };
+template <int S, class IX> struct RunsMinBlocks<WideRanker<S>, IX> { static constexpr int value = 8; };
+template <int SB, int KIND, class IT, int TPK, class IX> struct RunsMinBlocks<PoppyRanker<SB, KIND, IT, TPK>, IX> {
+    static constexpr int value = SB <= 512 && sizeof(IX) == 4 ? SBWT_RUNS_BLOCKS32_POPPY : SB <= 1024 ? 10 : 1;
 };
 constexpr u32 kStart = 0xfffffffeu; // lane state: start the run's current k-mer
 
@@ -465,8 +480,11 @@ struct RunEntry {
 // (the learned-Bloom sandwich: rejected by the model and by the backup Bloom
 // filter over the indexed k-mers the model rejects, so never a present one),
 // and the walk goes on with the k-mer to its left.
-template <class R, bool STREAM, bool FILTER, u32 WIN>
-__global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kernel(const R rk, const SearchArgs a) {
+//
+// IX: the type of the k-mer and letter indices the lanes carry (u32 when the
+// batch's letters, k-mers and rows stay below 2^32 - 2^16, run32_ok; else u64).
+template <class R, bool STREAM, bool FILTER, u32 WIN, class IX>
+__global__ void __launch_bounds__(128, RunsMinBlocks<R, IX>::value) search_runs_kernel(const R rk, const SearchArgs a) {
     static_assert(sizeof(typename R::IT) == 4, "the run form serves 32-bit intervals");
     static_assert(WIN % 32 == 0, "windows cover whole bitmap words");
     __shared__ RunEntry queue[kQueueWarps][kQueue];
@@ -481,7 +499,7 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
     const u32 C0 = (u32)a.C[0], C1 = (u32)a.C[1], C2 = (u32)a.C[2], C3 = (u32)a.C[3];
     const u32 rootR = (u32)(a.C[4] - 1ull);
     const PT *pre = reinterpret_cast<const PT *>(a.pre);
-    const u64 n_eff = min(a.n_kmers, a.kstart[a.n_rows]);
+    const IX n_eff = (IX)min(a.n_kmers, a.kstart[a.n_rows]);
     uint32_t *const member = a.member;
     RunEntry *q = queue[warp];
 #if SBWT_ANSWER_WRITE_ONCE
@@ -491,8 +509,9 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
 
     u32 head = 0, tail = 0;  // warp-uniform
     bool more = true;
-    u64 pj = 0, pe = 0, prow = 0;  // this lane's window: next k-mer to cut, end, row of pj
-    u64 kmer = 0, J = 0, pos = 0;  // current k-mer of this lane's run
+    IX pj = 0, pe = 0, prow = 0;  // this lane's window: next k-mer to cut, end, row of pj
+    u64 kmer = 0;                 // current k-mer of this lane's run:
+    IX J = 0, pos = 0;            // its index and letter offset
     u32 left = 0;                  // k-mers of the run left of J
     u32 L = 0, Rr = 0, I = kDone;
     u32 V = dev::kNoNode;          // STREAM: node of the k-mer right of J (found), or kNoNode
@@ -509,17 +528,17 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
                 if (base >= n_eff) {
                     more = false;
                 } else {
-                    const u64 end = min((u64)base + 32u * WIN, n_eff);
+                    const IX end = (IX)min((u64)base + 32u * WIN, (u64)n_eff);
 #if !SBWT_ANSWER_WRITE_ONCE
                     if (a.answers)  // NULL: membership bitmap only
                         for (u64 t = base + lane; t < end; t += 32u) a.answers[t] = ~0ull;
 #endif
-                    pj = min((u64)base + (u64)lane * WIN, end);
+                    pj = (IX)min((u64)base + (u64)lane * WIN, (u64)end);
                     pe = min(pj + WIN, end);
                     if (pj < pe) {
                         prow = a.chunk_row[pj / WIN];
                         if (member)
-                            for (u64 w = pj / 32u; w < (pe + 31u) / 32u; w++) member[w] = 0u;
+                            for (IX w = pj / 32u; w < (pe + 31u) / 32u; w++) member[w] = 0u;
                     }
                 }
                 __syncwarp();
@@ -529,7 +548,7 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
                 RunEntry e;
                 if (emit) {
                     while (a.kstart[prow + 1] <= pj) prow++;  // rows shorter than k hold no k-mers
-                    const u64 last = min(pe, a.kstart[prow + 1]) - 1u;
+                    const IX last = (IX)(min((u64)pe, a.kstart[prow + 1]) - 1u);
                     e.pos = a.row_starts[prow] + (last - a.kstart[prow]);
                     e.j = last;
                     e.len = (u32)(last - pj + 1u);
@@ -550,8 +569,8 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
         const u32 rank = __popc(m & lt);
         if (need && rank < take) {
             const RunEntry &e = q[(head + rank) & (kQueue - 1)];
-            pos = e.pos;
-            J = e.j;
+            pos = (IX)e.pos;
+            J = (IX)e.j;
             left = e.len - 1u;
             I = kStart;
             V = dev::kNoNode;
@@ -575,7 +594,7 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R>::value) search_runs_kern
                 n_skip++;
             } else {
                 // ---- start: letters (search_kernel.hpp:66-68) and presearch entry (:71-82)
-                const u64 b = min(pos, a.max_pos) << 1;
+                const u64 b = min((u64)pos, a.max_pos) << 1;
                 const u64 w0 = a.words[b >> 6], w1 = a.words[(b >> 6) + 1];
                 const u32 sh = (u32)(b & 63u);
                 kmer = (w0 << sh) | (shr_clamp(w1, 63u - sh) >> 1);
@@ -709,12 +728,28 @@ int launch_one(const R &rk, SearchArgs &a, const sbwt_index *ix, cudaStream_t s,
     return 0;
 }
 
+// The batch fits the 32-bit form of the walk: every k-mer index, letter
+// offset and row index with a window's slack below 2^32 (a letter offset
+// read from a bad row table is still clamped to max_pos).  SBWT_RUN_INDEX64=1
+// in the environment when an index is created keeps its walks on the 64-bit
+// form.
+bool run32_ok(const SearchArgs &a) {
+    const u64 lim = (1ull << 32) - (1ull << 16);
+    return !a.index64 && a.n_kmers < lim && a.max_pos < lim && a.n_rows < lim;
+}
+
+template <class R, u32 WIN, class IX>
+auto runs_kernel_ix(const SearchArgs &a) {
+    if constexpr (std::is_same<R, LinesRankerT<1>>::value) {  // the prefiltered walk: line layout only
+        if (a.reject)
+            return a.stream ? search_runs_kernel<R, true, true, WIN, IX> : search_runs_kernel<R, false, true, WIN, IX>;
+    }
+    return a.stream ? search_runs_kernel<R, true, false, WIN, IX> : search_runs_kernel<R, false, false, WIN, IX>;
+}
+
 template <class R, u32 WIN>
 auto runs_kernel(const SearchArgs &a) {
-    if constexpr (std::is_same<R, LinesRankerT<1>>::value) {  // the prefiltered walk: line layout only
-        if (a.reject) return a.stream ? search_runs_kernel<R, true, true, WIN> : search_runs_kernel<R, false, true, WIN>;
-    }
-    return a.stream ? search_runs_kernel<R, true, false, WIN> : search_runs_kernel<R, false, false, WIN>;
+    return run32_ok(a) ? runs_kernel_ix<R, WIN, u32>(a) : runs_kernel_ix<R, WIN, u64>(a);
 }
 
 template <class R>

@@ -431,6 +431,19 @@ def _row_mixture(rng, genome, k):
 def test_run_walk_modes_equal_per_kmer_search(cuda, k, p, layout):
     """The right-to-left run walk (absent-run skip, and skip + backward steps) answers
     exactly as the per-k-mer search and the oracle, bitmap included."""
+    _check_run_walk(cuda, k, p, layout)
+
+
+@pytest.mark.parametrize("k,p", [(31, 10), (5, 3), (32, 12)])
+@pytest.mark.parametrize("layout", [sg.SBWT_LAYOUT_LINES, sg.SBWT_LAYOUT_POPPY, sg.SBWT_LAYOUT_LINES512])
+def test_run_walk_64bit_index_form(cuda, monkeypatch, k, p, layout):
+    """Batches below 4G letters walk with 32-bit k-mer and letter indices; larger ones with
+    64-bit indices.  SBWT_RUN_INDEX64=1 puts a small batch on the 64-bit form."""
+    monkeypatch.setenv("SBWT_RUN_INDEX64", "1")
+    _check_run_walk(cuda, k, p, layout)
+
+
+def _check_run_walk(cuda, k, p, layout):
     rng = wl.rng_for(2000 + k * 17 + p)
     genome = wl.random_bases(rng, 60_000)
     built = sg.build_sbwt([genome.tobytes()], k)
