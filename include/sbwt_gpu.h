@@ -257,6 +257,7 @@ int sbwt_search_reads_noalloc(sbwt_index *index, const uint8_t *d_letters, uint6
  * threads a share of the chunks (sbwt_pipeline_dense_share) comes back as
  * u64 answers by DMA into a pinned answer buffer instead; environment:
  * SBWT_PIPELINE_TRANSFER=dense|sparse|hybrid forces one form,
+ * SBWT_PIPELINE_DENSE_SHARE=f sets the share of dense chunks,
  * SBWT_PIPELINE_CHUNK_LETTERS sets the chunk size (default 64M letters).
  * Replaces the
  * parse/position/search/copy-back chain of KmerSearch::search
@@ -290,10 +291,10 @@ int sbwt_set_host_threads(sbwt_index *index, int threads);
  * cross PCIe as such (the rest come back as bitmap + found node ids and are
  * expanded by the host threads), for an index of n_columns searched with
  * host_threads threads (0: the OpenMP default): 0 with six or more threads,
- * D / (D + T E) below (D = 57 GB/s of copies, E = 11 GB/s of expansion per
- * thread, T threads), 1 for indexes of 2^32 columns or more; the
- * SBWT_PIPELINE_TRANSFER override included.  Needs no GPU.  No reference
- * counterpart. */
+ * below that the measured best share (0.7 for 1-2 threads, 0.5 for 3, 0.3
+ * for 4, 0.15 for 5), 1 for indexes of 2^32 columns or more; the
+ * SBWT_PIPELINE_TRANSFER and SBWT_PIPELINE_DENSE_SHARE overrides included.
+ * Needs no GPU.  No reference counterpart. */
 double sbwt_pipeline_dense_share(uint64_t n_columns, int host_threads);
 
 /* Bytes the last sbwt_search_reads_host or sbwt_search_reads_host_member

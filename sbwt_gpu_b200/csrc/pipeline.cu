@@ -88,22 +88,23 @@ constexpr u32 kGroupWarps = 4;  // groups (warps) per block of group_nodes_kerne
 
 // How a chunk's answers cross PCIe: u64 answers (dense), the sparse form, or
 // both (split: some chunks dense, copied straight into the caller's pinned
-// buffer by the copy engines while the host threads expand the sparse
-// ones).  Sparse needs 32-bit node ids.  With T host threads the expansion
-// writes about kExpandPerThread bytes of answers per second per thread, the
-// copy engines kDmaBytes: with many threads (T >= kMinExpandThreads) every
-// chunk is sparse (the copy engines' writes into host memory would only
-// contend with the expansion's, measured slower); with fewer, the share of
-// dense chunks that lets both finish together, f = D / (D + T x E), spread
-// evenly over the chunks (2 threads, as under torchrun with 8 ranks on 16
-// cores: 72 % dense, about 1.4x the all-dense time; 1 thread: 84 %).  The
-// environment variable SBWT_PIPELINE_TRANSFER = dense | sparse | hybrid
-// (every fourth chunk dense) overrides the choice, and
-// SBWT_PIPELINE_DENSE_SHARE = f in [0, 1] sets the share itself.
+// buffer by the copy engines while the expander thread expands the sparse
+// ones).  Sparse needs 32-bit node ids.  The share of dense chunks per host
+// thread count T is the measured optimum (large workload, 16-core host,
+// sweep of T x share through sbwt_search_reads_host): the all-dense form
+// runs at 6.1G k-mers/s whatever T (49 GB/s of copies), all-sparse at 3.0G /
+// 5.7G / 8.2G / 12.5G for T = 2 / 3 / 4 / 6 (about 23 GB/s of expansion per
+// expanding thread, T - 1 of them); the best split was 0.7 at T <= 2 (6.6G),
+// 0.5 at T = 3 (8.3G), 0.3 at T = 4 (10.2G) and none from T = 6 (12.5G);
+// T = 5 takes 0.15, between its neighbours.  The copy engines' writes into
+// host memory slow the expansion down, so the optimum lies below the share
+// that a plain rate model gives.  The environment variable
+// SBWT_PIPELINE_TRANSFER = dense | sparse | hybrid (every fourth chunk
+// dense) overrides the choice, and SBWT_PIPELINE_DENSE_SHARE = f in [0, 1]
+// sets the share itself.
 enum Transfer { kDense, kSparse, kSplit };
 constexpr int kMinExpandThreads = 6;
-constexpr double kExpandPerThread = 11e9;  // bytes of u64 answers per second per host thread (measured)
-constexpr double kDmaBytes = 57e9;         // device->host copy, bytes per second (measured)
+constexpr double kDenseShare[kMinExpandThreads] = {0.7, 0.7, 0.7, 0.5, 0.3, 0.15};  // by T (T = 0 as 1)
 
 int host_threads(const sbwt_index *ix) { return ix->host_threads > 0 ? ix->host_threads : omp_get_max_threads(); }
 
@@ -125,7 +126,7 @@ double dense_share(u64 n, int T, Transfer *mode) {
     } else if (T >= kMinExpandThreads) {
         t = kSparse, f = 0.0;
     } else {
-        t = kSplit, f = kDmaBytes / (kDmaBytes + T * kExpandPerThread);
+        t = kSplit, f = kDenseShare[T < 0 ? 0 : T];
     }
     if (mode) *mode = t;
     return f;

@@ -97,7 +97,9 @@ def test_answer_transfer_degrades_with_the_per_rank_thread_split(monkeypatch):
     """Under torchrun each rank of this project's arm gets cores / ranks host threads; with 8 ranks on a
     16-core node that is 2.  The host pipeline then sends the share of chunks that lets the copy engines
     and the 2 expanding threads finish together as u64 answers (72 %), not every chunk (the all-dense form,
-    PCIe-bound) and not none (2 threads would expand far slower than PCIe copies)."""
+    PCIe-bound) and not none (2 threads would expand far slower than PCIe copies).  The shares are the
+    measured optima of a sweep on the GPU box (large workload, 16 cores): 0.7 at 2 threads gave 6.6G
+    k-mers/s against 6.1G all-dense and 3.0G all-sparse."""
     import bench as b
     import sbwt_gpu_b200 as sg
     monkeypatch.delenv("SBWT_PIPELINE_TRANSFER", raising=False)
@@ -109,14 +111,14 @@ def test_answer_transfer_degrades_with_the_per_rank_thread_split(monkeypatch):
     t = int(os.environ["OMP_NUM_THREADS"])
     assert t == 2
     f = sg.pipeline_dense_share(n, t)
-    assert 0.6 < f < 0.8
-    # the modelled time of the split is below both pure forms: dense DMA 57 GB/s, expansion 11 GB/s a thread
-    dense_t, expand_t = 1 / 57.0, 1 / (11.0 * t)
-    split_t = max(f * dense_t, (1 - f) * expand_t)
-    assert split_t < 0.8 * dense_t and split_t < expand_t
+    assert f == pytest.approx(0.7)
+    assert [sg.pipeline_dense_share(n, x) for x in (3, 4, 5)] == pytest.approx([0.5, 0.3, 0.15])
+    monkeypatch.setenv("SBWT_PIPELINE_DENSE_SHARE", "0.42")
+    assert sg.pipeline_dense_share(n, 2) == pytest.approx(0.42)
+    monkeypatch.delenv("SBWT_PIPELINE_DENSE_SHARE")
     # more threads: all sparse; fewer: a larger dense share; indexes past 2^32 columns: all dense
     assert sg.pipeline_dense_share(n, 16) == 0.0 and sg.pipeline_dense_share(n, 6) == 0.0
-    assert sg.pipeline_dense_share(n, 1) > f > sg.pipeline_dense_share(n, 4) > 0.0
+    assert sg.pipeline_dense_share(n, 1) >= f > sg.pipeline_dense_share(n, 4) > 0.0
     assert sg.pipeline_dense_share(1 << 33, 16) == 1.0
     monkeypatch.setenv("SBWT_PIPELINE_TRANSFER", "sparse")
     assert sg.pipeline_dense_share(n, 2) == 0.0
