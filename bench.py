@@ -383,11 +383,10 @@ def kernel_traffic(kernel, workload, n_kmers):
 
 def table_sizes(n_columns, p, stream_tables=True):
     """Bytes of the index structures the run walk gathers from: presearch table (8-byte entries below
-    2^32 columns), backward table (4 bytes per column below 2^28 columns, else 8) and the 32-byte lines of
-    the four vectors."""
+    2^32 columns), backward table (8 bytes per column) and the 32-byte lines of the four vectors."""
     lpc = (n_columns // 224 + 1 + 7) // 8 * 8
     return {"presearch": (1 << (2 * p)) * (8 if n_columns < (1 << 32) else 16) if p else 0,
-            "backward_table": (4 if n_columns < (1 << 28) else 8) * n_columns if stream_tables else 0,
+            "backward_table": 8 * n_columns if stream_tables else 0,
             "lines": 4 * lpc * 32}
 
 

@@ -327,7 +327,6 @@ extern "C" void sbwt_index_free(sbwt_index *ix) {
     cudaFree(ix->d_node);
     cudaFree(ix->d_sel);
     cudaFree(ix->d_back);
-    cudaFree(ix->d_back32);
     for (int i = 0; i < sbwt_index::kPipeSlots; i++) {
         ix->ws[i].release();
         if (ix->pipe_stream[i]) cudaStreamDestroy(ix->pipe_stream[i]);
@@ -537,7 +536,7 @@ void l2_setaside_release(sbwt_index *ix) {
 void set_gather_policies(const sbwt_index *ix, SearchArgs &a) {
     const u64 half = ix->l2_bytes / 2;
     const u64 pre_bytes = ix->p ? (1ull << (2 * ix->p)) * (ix->pre64 ? 16ull : 8ull) : 0;
-    const u64 back_bytes = ix->d_back ? ix->n * 8ull : ix->d_back32 ? ix->n * 4ull : 0;
+    const u64 back_bytes = ix->d_back ? ix->n * 8ull : 0;
     const int ev = ix->shape.evict;
     a.ef_pre = a.runs && ev != 1 && (ev == 2 || pre_bytes > half);
     a.ef_back = a.runs && ev != 1 && (ev == 2 || back_bytes > half);

@@ -143,19 +143,6 @@ __device__ __forceinline__ u64 ld_gather_u64(const u64 *p, bool ef, u64 pol) {
     return __ldg(reinterpret_cast<const unsigned long long *>(p));
 }
 
-__device__ __forceinline__ u32 ld_gather_u32(const u32 *p, bool ef, u64 pol) {
-#if SBWT_GATHER_EVICT_FIRST
-    if (ef) {
-        u32 v;
-        asm(SBWT_GATHER_LD ".L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
-        return v;
-    }
-#endif
-    (void)ef;
-    (void)pol;
-    return __ldg(p);
-}
-
 // x >> s with the PTX rule that s >= 64 gives 0 (the reference relies on it,
 // include/gpu/rank_kernel.hpp:218,226-229).
 __device__ __forceinline__ u64 shr_clamp(u64 x, u32 s) {

@@ -145,8 +145,7 @@ struct sbwt_index {
     // backward-step structures (stream.cu): node nibbles, select samples, backward table
     uint8_t *d_node = nullptr;
     uint32_t *d_sel = nullptr;
-    uint64_t *d_back = nullptr;  // backward table (stream.cuh, SBWT_BACK_TABLE), 8 bytes an entry
-    uint32_t *d_back32 = nullptr;  // or 4 bytes an entry, below 2^28 nodes
+    uint64_t *d_back = nullptr;  // backward table (stream.cuh, SBWT_BACK_TABLE)
     uint32_t sel_off[4] = {0, 0, 0, 0}, sel_n[4] = {0, 0, 0, 0};
     bool stream_ok = false;
     // device ms of the last build of: lines, poppy, presearch table, backward-step structures

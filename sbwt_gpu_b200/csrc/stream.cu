@@ -12,7 +12,6 @@
 //   code(v) = sum_t lastletter(pred^t(v)) << 2t,  len(v) = letters before the root
 // Then first letter = letter k-1 (or $ if len < k), and v starts a group iff
 // its last k-1 letters (and how many of them are real) differ from v-1's.
-#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -111,29 +110,6 @@ __global__ void back_table_kernel(const StreamView sv, u64 *__restrict__ back) {
     back[v] = e;
 }
 
-// The same in 4 bytes an entry (n < 2^28): (pred(v) + [$ in its group]) | letters A..T << 28.
-__global__ void back_table32_kernel(const StreamView sv, u32 *__restrict__ back) {
-    const u32 v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= sv.n) return;
-    u32 e = 0;
-    if (v) {
-        const u32 u0 = sv.pred(v);
-        if (u0 < sv.n) {
-            const u32 m = sv.group_letters(u0);
-            e = (u0 + (m & 1u)) | ((m >> 1) & 15u) << kBack32Bits;
-        }
-    }
-    back[v] = e;
-}
-
-// The 4-byte backward table: below 2^28 nodes, unless the environment
-// variable SBWT_BACK_TABLE32 is "0" when the structures are built.
-bool back_table32(const sbwt_index *ix) {
-    if (ix->n >= (1ull << kBack32Bits)) return false;
-    const char *e = std::getenv("SBWT_BACK_TABLE32");
-    return !(e && e[0] == '0' && e[1] == 0);
-}
-
 }  // namespace
 
 StreamView stream_view(const sbwt_index *ix) {
@@ -149,7 +125,6 @@ StreamView stream_view(const sbwt_index *ix) {
     }
     sv.node = ix->d_node;
     sv.back = ix->d_back;
-    sv.back32 = ix->d_back32;
     sv.n = (u32)ix->n;
     return sv;
 }
@@ -206,10 +181,7 @@ int build_stream(sbwt_index *ix, cudaStream_t s) {
             cur ^= 1;
         }
         node_nibbles_kernel<<<(n / 2 + 1 + 255) / 256, 256, 0, s>>>(n, ix->k, code[cur], len[cur], ix->d_node);
-        if (SBWT_BACK_TABLE && back_table32(ix)) {
-            e = cudaMalloc(&ix->d_back32, (size_t)n * sizeof(u32));
-            if (e == cudaSuccess) back_table32_kernel<<<blocks, 256, 0, s>>>(stream_view(ix), ix->d_back32);
-        } else if (SBWT_BACK_TABLE) {
+        if (SBWT_BACK_TABLE) {
             e = cudaMalloc(&ix->d_back, (size_t)n * sizeof(u64));
             if (e == cudaSuccess) back_table_kernel<<<blocks, 256, 0, s>>>(stream_view(ix), ix->d_back);
         }
@@ -230,11 +202,9 @@ int build_stream(sbwt_index *ix, cudaStream_t s) {
         cudaFree(ix->d_node);
         cudaFree(ix->d_sel);
         cudaFree(ix->d_back);
-        cudaFree(ix->d_back32);
         ix->d_node = nullptr;
         ix->d_sel = nullptr;
         ix->d_back = nullptr;
-        ix->d_back32 = nullptr;
         return rc;
     }
     ix->stream_ok = true;

@@ -15,9 +15,6 @@
 // first letter (0 = $, 1..4 = A..T) and a flag for the first node of its
 // group (bit 3); and the backward table: per node v, pred(v) with the set of
 // first letters of pred(v)'s group, so that a backward step is one load.
-// Below 2^28 nodes an entry takes 4 bytes (back32): the first member with
-// a letter, pred(v) + [the group has a $ member], in the low 28 bits and the
-// group's letters A..T in the top 4; else 8 bytes (back).
 // select_c uses the line counts plus a sample of the line holding every 64th
 // one.
 #pragma once
@@ -29,10 +26,9 @@ namespace dev {
 constexpr u32 kSelLog = 6;          // one select sample per 64 ones
 constexpr uint8_t kGroupStart = 8;  // node nibble: bit 3 = first node of its group
 constexpr u32 kNoNode = 0;          // node 0 (the all-$ root) is never a k-mer's node
-constexpr u32 kBack32Bits = 28;     // node bits of a 4-byte backward-table entry
 
-// Backward steps through the backward table (1) or through select + node
-// nibbles (0).
+// Backward steps through the 8-byte-per-column backward table (1) or through
+// select + node nibbles (0).
 #ifndef SBWT_BACK_TABLE
 #define SBWT_BACK_TABLE 1
 #endif
@@ -95,7 +91,6 @@ struct StreamView {
     u32 sel_n[4];
     const uint8_t *node;   // per node a nibble (first letter | kGroupStart), two per byte
     const u64 *back;       // backward table: per node pred(v) | group_letters(pred(v)) << 32
-    const u32 *back32;     // or, below 2^28 nodes: (pred(v) + [$ member]) | letters A..T << 28
     u32 n;                 // nodes
     u32 C[4];
 
@@ -128,12 +123,6 @@ struct StreamView {
     // load of v's entry u0 | group_letters(u0) << 32 (the backward table); the
     // member with first letter a sits after the members with smaller ones.
     __device__ __forceinline__ u32 back_step(u32 v, u32 a, bool ef, u64 pol) const {
-        if (back32) {
-            const u32 e = ld_gather_u32(back32 + v, ef, pol);
-            const u32 m = e >> kBack32Bits;
-            if (!((m >> a) & 1u)) return kNoNode;
-            return (e & ((1u << kBack32Bits) - 1u)) + (u32)__popc(m & ((1u << a) - 1u));
-        }
         const u64 e = ld_gather_u64(back + v, ef, pol);
         const u32 m = (u32)(e >> 32);
         if (!((m >> (a + 1u)) & 1u)) return kNoNode;

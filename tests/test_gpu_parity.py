@@ -436,15 +436,10 @@ def test_run_walk_modes_equal_per_kmer_search(cuda, k, p, layout):
 
 @pytest.mark.parametrize("k,p", [(31, 10), (5, 3), (32, 12)])
 @pytest.mark.parametrize("layout", [sg.SBWT_LAYOUT_LINES, sg.SBWT_LAYOUT_POPPY, sg.SBWT_LAYOUT_LINES512])
-@pytest.mark.parametrize("form", ["index64", "back_table64"])
-def test_run_walk_forms_of_large_inputs(cuda, monkeypatch, k, p, layout, form):
-    """The forms that only batches of 4G letters or more (64-bit k-mer and letter indices in the
-    walk) and indexes of 2^28 columns or more (8-byte backward-table entries) take, put on a small
-    case by SBWT_RUN_INDEX64=1 and SBWT_BACK_TABLE32=0."""
-    if form == "index64":
-        monkeypatch.setenv("SBWT_RUN_INDEX64", "1")
-    else:
-        monkeypatch.setenv("SBWT_BACK_TABLE32", "0")
+def test_run_walk_64bit_index_form(cuda, monkeypatch, k, p, layout):
+    """Batches below 4G letters walk with 32-bit k-mer and letter indices; larger ones with
+    64-bit indices.  SBWT_RUN_INDEX64=1 puts a small batch on the 64-bit form."""
+    monkeypatch.setenv("SBWT_RUN_INDEX64", "1")
     _check_run_walk(cuda, k, p, layout)
 
 
