@@ -67,6 +67,7 @@ def parse():
     ap.add_argument("--evict", type=int, default=-1, choices=[-1, 0, 1, 2],
                     help="evict-first gathers: 0 by table size, 1 never, 2 always (-1: default)")
     ap.add_argument("--l2-persist", type=int, default=-1, choices=[-1, 0, 1], help="rank lines in the L2 set-aside")
+    ap.add_argument("--blocks-per-sm", type=int, default=0, help="resident blocks per SM of the run walk (0: as many as fit)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-e2e", action="store_true")
@@ -553,9 +554,10 @@ def main():
               else ("search_queue_kernel" if args.kpt == 0 else "search_kernel"))
     if args.l2_fetch:
         ix.set_l2_fetch_granularity(args.l2_fetch)
-    if args.window or args.evict >= 0 or args.l2_persist >= 0:
+    if args.window or args.evict >= 0 or args.l2_persist >= 0 or args.blocks_per_sm:
         ix.set_walk_options(window=args.window or None, evict=args.evict if args.evict >= 0 else None,
-                            l2_persist=args.l2_persist if args.l2_persist >= 0 else None)
+                            l2_persist=args.l2_persist if args.l2_persist >= 0 else None,
+                            blocks_per_sm=args.blocks_per_sm or None)
     build_times = ix.build_times()  # device ms: rank words (lines), poppy, presearch, backward table
     info = ix.info()
 
