@@ -447,12 +447,12 @@ __device__ __forceinline__ void stage_absent(u64 *ans, u64 *slot, u64 x, u64 b, 
 // 10 for the poppy ranker with basic blocks of up to 256 bits (48 registers);
 // the larger poppy blocks keep the compiler's choice (a cap spills there).
 // The form with 32-bit k-mer and letter indices (IX = u32, batches below 4G
-// letters) needs 52-55 registers uncapped instead of 56 + 12 bytes of spill.
-// Measured on the large workload (p = 12 / 15): 9 blocks 8.25 / 7.32 ms
-// (the 64-bit form: 8.32 / 7.38), 10 blocks (48 registers, 20 bytes of
-// spill) 8.32 / 7.38, 12 blocks (40 registers, 82 bytes) 8.94 / 8.25.
+// letters), with C in shared memory, fits 10 blocks (48 registers, 8 bytes
+// of spill).  Measured on the large workload, p = 12: 7.99 ms against 8.26
+// at 9 blocks (the 64-bit form: 8.32); with C in registers 10 blocks spilled
+// 20 bytes and ran 8.32, 12 blocks (40 registers, 82 bytes) 8.94.
 #ifndef SBWT_RUNS_BLOCKS32
-#define SBWT_RUNS_BLOCKS32 9
+#define SBWT_RUNS_BLOCKS32 10
 #endif
 // The same for the poppy ranker with basic blocks of up to 512 bits (44-46
 // registers at 10 blocks, no spill): basic blocks of 512 bits, 10 blocks
@@ -496,7 +496,11 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R, IX>::value) search_runs_
     const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const u32 lt = (1u << lane) - 1u;
     const u32 k = a.k, p = a.p;
-    const u32 C0 = (u32)a.C[0], C1 = (u32)a.C[1], C2 = (u32)a.C[2], C3 = (u32)a.C[3];
+    // C in shared memory and the cache policy made at each gather: registers kept for the
+    // run state, so that the 32-bit form fits 10 blocks per SM
+    __shared__ u32 sC[4];
+    if (threadIdx.x < 4) sC[threadIdx.x] = (u32)a.C[threadIdx.x];
+    __syncthreads();
     const u32 rootR = (u32)(a.C[4] - 1ull);
     const PT *pre = reinterpret_cast<const PT *>(a.pre);
     const IX n_eff = (IX)min(a.n_kmers, a.kstart[a.n_rows]);
@@ -515,7 +519,6 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R, IX>::value) search_runs_
     u32 left = 0;                  // k-mers of the run left of J
     u32 L = 0, Rr = 0, I = kDone;
     u32 V = dev::kNoNode;          // STREAM: node of the k-mer right of J (found), or kNoNode
-    const u64 gpol = l2_evict_first_policy();  // for the gathers from tables too large for L2
     u32 n_skip = 0;                            // FILTER: k-mers answered from the reject bitmap
 
     for (;;) {
@@ -586,7 +589,7 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R, IX>::value) search_runs_
             if (STREAM && V != dev::kNoNode) {
                 // ---- backward step: k-mer J = x[J] . (first k-1 letters of k-mer J+1)
                 const u32 letter = (u32)(a.words[pos >> 5] >> (62u - 2u * (u32)(pos & 31u))) & 3u;
-                const u32 u = a.sv.back_step(V, letter, a.ef_back, gpol);
+                const u32 u = a.sv.back_step(V, letter, a.ef_back, l2_evict_first_policy());
                 adv = 1;
                 if (u != dev::kNoNode) found = u;
             } else if (FILTER && ((__ldg(a.reject + (J >> 5)) >> (J & 31u)) & 1u)) {
@@ -609,7 +612,7 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R, IX>::value) search_runs_
                         if (w == 0) L = 1u, Rr = 0u;
                     }
                     if (w == kPreEscape) {
-                        const PT e = ld_gather_u32x2(pre + idx, a.ef_pre, gpol);
+                        const PT e = ld_gather_u32x2(pre + idx, a.ef_pre, l2_evict_first_policy());
                         L = e.x;
                         Rr = e.y;
                     }
@@ -631,7 +634,7 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R, IX>::value) search_runs_
         if (I < k) {
             const u32 c = (u32)((kmer >> (62u - 2u * I)) & 3u);
             const typename R::Fetch f = rk.fetch(c, L, Rr, 0);
-            const u32 Cc = c == 0 ? C0 : c == 1 ? C1 : c == 2 ? C2 : C3;
+            const u32 Cc = sC[c];
             rk.finish(f, Cc, L, Rr, 0, kFull);
             I++;
             if (L > Rr) {
