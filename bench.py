@@ -900,7 +900,8 @@ def other_workloads(args, sg, orc, k, dev, stream, rank, world, local_rank):
         letters, rows = wl.mixed_reads(rrng, small, n_reads // 10, n_reads - n_reads // 10, 150, 0.01)
         plain = device_leg(ix, sg, orc, paths, letters, rows, k, 10, steps, 2, dev, stream, kern, None,
                            min(args.cpu_seconds, 2.0), "prefilter reads (small index)")
-        ox_ans = orc.OracleIndex.from_files(paths).search_reads(letters[: int(rows[2000])], rows[:2001], k, 10)
+        ns = min(2000, rows.size - 1)  # oracle sample: the first 2000 reads, or all of a small batch
+        ox_ans = orc.OracleIndex.from_files(paths).search_reads(letters[: int(rows[ns])], rows[: ns + 1], k, 10)
         pf_out["batched"] = filtered_leg(ix, pf, sg, letters, rows, k, steps, dev, stream, plain["value"],
                                          f"small index (1 Mbp, k=31, p=10); {n_reads} reads x 150 bp "
                                          "(10% genome-sampled with 1% subs, 90% uniform random)", ox_ans)
