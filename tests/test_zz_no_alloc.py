@@ -4,7 +4,7 @@ already holds, or an application that accounts for every device allocation
 itself).  Its scratch is a fixed device array inside the library instead of
 buffers grown with cudaMalloc.
 
-Checked through the C ABI against sbwt_search_reads on the same batch, on two
+Checked through the C ABI against sbwt_search_reads and the oracle on the same batch, on two
 calls in a row (the array keeps the previous call's contents, so the second
 call shows that nothing stale leaks into its answers), in the default run walk
 and with every k-mer searched, on the line and the poppy layouts, with answers
@@ -17,6 +17,7 @@ from ctypes import c_void_p
 import numpy as np
 import pytest
 
+import oracle as orc
 import sbwt_gpu_b200 as sg
 from sbwt_gpu_b200 import _lib, workloads as wl
 
@@ -43,6 +44,7 @@ def test_noalloc_search_equals_search_reads(cuda, layout, mode):
     kw = dict(k=31, k_presearch=10, search_mode=sg.SEARCH_STREAM if mode == "stream" else sg.SEARCH_EVERY_KMER)
     if layout == "poppy":
         kw.update(layout=sg.SBWT_LAYOUT_POPPY, bits_in_superblock=1024)
+    ox = orc.OracleIndex(built.bits, built.n_bits)
     with sg.Index.from_bits(built.bits, built.n_bits, **kw) as ix:
         for letters, rows in batches:
             nk = sg.count_kmers(rows, 31)
@@ -57,6 +59,8 @@ def test_noalloc_search_equals_search_reads(cuda, layout, mode):
             torch.cuda.synchronize()
             assert torch.equal(got, want)
             assert torch.equal(got_bits, want_bits)
+            # and against the oracle itself, so that a fault shared with sbwt_search_reads shows too
+            assert np.array_equal(got.cpu().numpy().view(np.uint64), ox.search_reads(letters, rows, 31, 10))
             # membership only: no answer array
             only_bits = torch.full(((nk + 31) // 32,), -1, dtype=torch.int32, device=cuda)
             assert _noalloc(ix, d_l, d_r, None, nk, only_bits) == 0, _lib.lib.sbwt_last_error()
