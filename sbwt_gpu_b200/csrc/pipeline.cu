@@ -450,7 +450,9 @@ int pipeline_chunks(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, 
             SBWT_TRY(grow_host(w.h_nodes, w.h_nodes_cap, max_k + 32));  // slack: expand_answers may read one past
         }
     }
-    if (member) std::memset(member, 0, (n_kmers + 31) / 32 * sizeof(uint32_t));
+    // member: each output word is assigned by the first chunk that reaches it and or-ed by the
+    // next one where a chunk starts inside a word (chunks are drained in order), so the
+    // output needs no clearing pass first
     // pending[i]: chunk whose results sit in slot i's pinned staging (or are
     // on their way there); stage[i]: 0 idle, 1 issued, 2 (sparse) node ids
     // requested
@@ -500,15 +502,18 @@ int pipeline_chunks(sbwt_index *ix, const uint8_t *letters, uint64_t n_letters, 
                 const u64 nw = (c.nk + 31) / 32, w0 = c.k0 >> 5;
                 const u32 sh = (u32)(c.k0 & 31u);
                 const u64 out_words = (n_kmers + 31) / 32;
+                uint32_t *dst = member + w0;
                 if (sh == 0) {
-                    for (u64 i = 0; i < nw; i++) member[w0 + i] |= src[i];
+#pragma omp parallel for schedule(static) if (nw > (1u << 16))
+                    for (int64_t i = 0; i < (int64_t)nw; i++) dst[i] = src[i];
                 } else {
-                    // word w0+i gets the high part of src[i-1] and the low part of src[i]
-                    uint32_t *dst = member + w0;
+                    // word w0 already holds the previous chunk's low bits; word w0+i gets the high
+                    // part of src[i-1] and the low part of src[i]; word w0+nw (if any) is the next
+                    // chunk's first word, assigned here and or-ed by it
                     dst[0] |= src[0] << sh;
 #pragma omp parallel for schedule(static) if (nw > (1u << 16))
-                    for (int64_t i = 1; i < (int64_t)nw; i++) dst[i] |= (src[i] << sh) | (src[i - 1] >> (32u - sh));
-                    if (w0 + nw < out_words) dst[nw] |= src[nw - 1] >> (32u - sh);
+                    for (int64_t i = 1; i < (int64_t)nw; i++) dst[i] = (src[i] << sh) | (src[i - 1] >> (32u - sh));
+                    if (w0 + nw < out_words) dst[nw] = src[nw - 1] >> (32u - sh);
                 }
             }
             pending[slot] = -1;

@@ -588,7 +588,7 @@ def test_host_answers_sparse_transfer_many_chunks(small, cuda, monkeypatch, chun
     rows[1:] = np.cumsum([p.size for p in parts])
     want = orc.OracleIndex(b.bits, b.n_bits).search_reads(letters, rows, k, 10)
     monkeypatch.setenv("SBWT_PIPELINE_CHUNK_LETTERS", str(chunk))
-    if transfer == "threads2":  # two host threads: the split by sbwt_pipeline_dense_share (72 % of chunks dense)
+    if transfer == "threads2":  # two host threads: the split by sbwt_pipeline_dense_share (70 % of chunks dense)
         monkeypatch.delenv("SBWT_PIPELINE_TRANSFER", raising=False)
     else:
         monkeypatch.setenv("SBWT_PIPELINE_TRANSFER", transfer)
@@ -601,6 +601,9 @@ def test_host_answers_sparse_transfer_many_chunks(small, cuda, monkeypatch, chun
         ix.search_reads_host(letters, rows, pa)
         moved_pinned = ix.pipeline_bytes()
         mem = ix.member_reads_host(letters, rows)
+        junk = np.full(mem.size, 0xA5A5A5A5, dtype=np.uint32)  # every output word is written, none or-ed into stale bits
+        ix.member_reads_host(letters, rows, junk)
+    assert np.array_equal(junk, mem)
     assert letters.size > 2 * chunk
     assert moved["h2d"] > letters.size and 0 < moved["d2h"]
     assert (moved["d2h"] >= 8 * want.size) == (transfer == "dense")
