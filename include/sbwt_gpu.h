@@ -203,9 +203,10 @@ int sbwt_use_graphs(sbwt_index *index, int on);
  * runs past n_kmers.  In the run-walking search modes, k-mers at consecutive
  * positions (each position one more than the one before, as the reference's
  * positions of one read are) are walked as runs, as sbwt_search_reads does;
- * the call then waits once on `stream` (the run count sizes the run table),
- * and positions with runs shorter than four k-mers on average are searched
- * one k-mer at a time. */
+ * positions with runs shorter than four k-mers on average are searched one
+ * k-mer at a time.  The choice is made on the device, so the call is
+ * stream-ordered with no host wait; the handle's run table is sized for a
+ * quarter of the k-mers (4 bytes per k-mer of device memory). */
 int sbwt_search_packed(sbwt_index *index, const uint64_t *d_kmer_string, uint64_t n_words,
                        uint64_t *d_positions_in_results_out, uint64_t n_kmers, void *stream);
 

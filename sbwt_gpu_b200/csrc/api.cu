@@ -699,28 +699,29 @@ extern "C" int sbwt_search_packed(sbwt_index *ix, const uint64_t *d_kmer_string,
     cudaStream_t s = (cudaStream_t)stream;
     Workspace &w = ix->ws[0];
     SBWT_TRY(grow(w.counter, w.counter_cap, 1));
+    const u64 *runs_dev = nullptr;
     if (runs_form(ix)) {
-        // runs of consecutive positions go to the run-walking kernel (packed_runs.cu)
-        u64 n_rows = 0;
+        // runs of consecutive positions go to the run-walking kernel (packed_runs.cu); the run
+        // count stays on the device, and of the two launches below only the one it chose searches
         SearchArgs a = base_args(ix, true);
-        SBWT_TRY(packed_runs(w, d_positions_in_results_out, n_kmers, a.chunk, s, &n_rows));
-        if (n_rows) {
-            a.words = d_kmer_string;
-            a.positions = nullptr;
-            a.row_starts = w.rows;
-            a.kstart = w.kstart;
-            a.chunk_row = w.chunk_row;
-            a.n_rows = n_rows;
-            a.max_pos = (n_words - 1) * 32 - 1;
-            a.answers = d_positions_in_results_out;
-            a.n_kmers = n_kmers;
-            a.counter = w.counter;
-            return launch_search(ix, a, s, nullptr);
-        }
+        SBWT_TRY(packed_runs(w, d_positions_in_results_out, n_kmers, a.chunk, s, &runs_dev));
+        a.words = d_kmer_string;
+        a.positions = nullptr;
+        a.row_starts = w.rows;
+        a.kstart = w.kstart;
+        a.chunk_row = w.chunk_row;
+        a.runs_dev = runs_dev;
+        a.n_rows = n_kmers / kMinRunKmers;  // the most runs the walk takes (its index-width choice)
+        a.max_pos = (n_words - 1) * 32 - 1;
+        a.answers = d_positions_in_results_out;
+        a.n_kmers = n_kmers;
+        a.counter = w.counter;
+        SBWT_TRY(launch_search(ix, a, s, nullptr));
     }
     SearchArgs a = base_args(ix, false);
     a.words = d_kmer_string;
     a.positions = d_positions_in_results_out;
+    a.runs_dev = runs_dev;
     a.max_pos = (n_words - 1) * 32 - 1;
     a.answers = d_positions_in_results_out;
     a.n_kmers = n_kmers;

@@ -36,6 +36,9 @@ struct SearchArgs {
     const u64 *kstart;      // read mode: first k-mer index of each row (n_rows + 1)
     const u32 *chunk_row;   // read mode: row of the first k-mer of each chunk
     u64 n_rows;             // read mode: rows (kstart[n_rows] = k-mers in the batch)
+    const u64 *runs_dev;    // kernel contract: the run count on the device, or NULL.  The run walk
+                            // takes it as n_rows and searches only when the runs are usable
+                            // (runs_usable); the per-k-mer kernels search only when they are not
     u64 max_pos;            // largest letter offset whose 64-bit window lies inside `words`
     u64 *answers;
     u64 n_kmers;
@@ -211,7 +214,11 @@ int build_stream(sbwt_index *ix, cudaStream_t s);
 dev::StreamView stream_view(const sbwt_index *ix);
 
 // packed_runs.cu
-int packed_runs(Workspace &w, const u64 *positions, u64 n_kmers, u32 chunk, cudaStream_t s, u64 *n_rows);
+// The kernel contract's runs are walked when they average at least
+// kMinRunKmers k-mers (fewer: random positions, searched one by one).
+constexpr u64 kMinRunKmers = 4;
+__host__ __device__ inline bool runs_usable(u64 runs, u64 n_kmers) { return runs != 0 && runs * kMinRunKmers <= n_kmers; }
+int packed_runs(Workspace &w, const u64 *positions, u64 n_kmers, u32 chunk, cudaStream_t s, const u64 **runs_dev);
 
 // api.cu
 // Launch arguments of a search with the index's current shape and mode (the

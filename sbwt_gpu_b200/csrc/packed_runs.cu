@@ -10,7 +10,11 @@
 // become a row table (first k-mer index and letter offset of each run), after
 // which the search is the one of sbwt_search_reads, writing its answers over
 // the positions.  When the runs are short (random positions) the per-k-mer
-// search is used instead.
+// search is used instead.  The choice is made on the device: the run count
+// never comes back to the host, the run table is sized for the most runs the
+// walk takes (a quarter of the k-mers), both searches are launched and each
+// returns at once unless it is the one the count chose, so a call is
+// stream-ordered with no host wait.
 #include <cub/cub.cuh>
 
 #include "internal.h"
@@ -68,9 +72,12 @@ __global__ void __launch_bounds__(kThreads) start_bits_kernel(const u64 *__restr
 // before it) - 1.
 __global__ void __launch_bounds__(kWords) run_table_kernel(const u64 *__restrict__ pos, u64 n,
                                                            const uint32_t *__restrict__ bits,
-                                                           const u64 *__restrict__ block_offset, u64 n_rows,
-                                                           u32 chunk_words, u64 *__restrict__ kstart,
-                                                           u64 *__restrict__ row_start, u32 *__restrict__ chunk_row) {
+                                                           const u64 *__restrict__ block_offset,
+                                                           const u64 *__restrict__ runs_dev, u32 chunk_words,
+                                                           u64 *__restrict__ kstart, u64 *__restrict__ row_start,
+                                                           u32 *__restrict__ chunk_row) {
+    const u64 n_rows = *runs_dev;
+    if (!runs_usable(n_rows, n)) return;  // the per-k-mer search takes this call
     __shared__ u32 warp_tot[kWords / 32];
     const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const u64 w = (u64)blockIdx.x * kWords + threadIdx.x;
@@ -99,37 +106,35 @@ __global__ void __launch_bounds__(kWords) run_table_kernel(const u64 *__restrict
 
 }  // namespace
 
-// Builds the run table of `positions` into w.kstart (n_rows + 1 entries),
-// w.rows (n_rows row starts) and w.chunk_row (the run of every chunk-th
-// k-mer; chunk a multiple of 32); *n_rows = 0 when the runs average fewer
-// than four k-mers (the caller then searches every k-mer).  Synchronises s
-// once (the run count comes back to the host to size the tables).
-int packed_runs(Workspace &w, const u64 *positions, u64 n_kmers, u32 chunk, cudaStream_t s, u64 *n_rows) {
-    *n_rows = 0;
+// Builds the run table of `positions` into w.kstart (runs + 1 entries),
+// w.rows (runs row starts) and w.chunk_row (the run of every chunk-th k-mer;
+// chunk a multiple of 32), where runs = *runs_dev, the run count, left on the
+// device; when runs_usable(runs, n_kmers) is false nothing is written and the
+// per-k-mer search takes the call.  No host wait.
+int packed_runs(Workspace &w, const u64 *positions, u64 n_kmers, u32 chunk, cudaStream_t s, const u64 **runs_dev) {
+    *runs_dev = nullptr;
     if (chunk == 0 || chunk % 32u) return set_error("run chunks must be whole bitmap words");
     const u64 nb = (n_kmers + kBlockItems - 1) / kBlockItems;
-    // w.scan: block counts (then their exclusive scan, in place), the scan's scratch, the start bitmap
+    // w.scan: block counts (then their exclusive scan, in place; the total at counts[nb]), the
+    // scan's scratch, the start bitmap
     size_t tmp_bytes = 0;
     SBWT_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, w.scan, w.scan, (int64_t)nb + 1, s));
     const u64 tmp_words = tmp_bytes / sizeof(u64) + 1;
     SBWT_TRY(grow(w.scan, w.scan_cap, nb + 1 + tmp_words + nb * (kWords / 2)));
+    const u64 max_runs = n_kmers / kMinRunKmers;
+    SBWT_TRY(grow(w.kstart, w.kstart_cap, max_runs + 1));
+    SBWT_TRY(grow(w.rows, w.rows_cap, max_runs + 1));
+    SBWT_TRY(grow(w.chunk_row, w.chunk_cap, (n_kmers + chunk - 1) / chunk));
     u64 *counts = w.scan, *tmp = w.scan + nb + 1;
     uint32_t *bits = reinterpret_cast<uint32_t *>(tmp + tmp_words);
     SBWT_CHECK_CUDA(cudaMemsetAsync(counts + nb, 0, sizeof(u64), s));
     start_bits_kernel<<<(unsigned)nb, kThreads, 0, s>>>(positions, n_kmers, bits, counts);
     SBWT_CHECK_CUDA(cudaGetLastError());
     SBWT_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, counts, counts, (int64_t)nb + 1, s));
-    u64 runs = 0;
-    SBWT_CHECK_CUDA(cudaMemcpyAsync(&runs, counts + nb, sizeof runs, cudaMemcpyDeviceToHost, s));
-    SBWT_CHECK_CUDA(cudaStreamSynchronize(s));
-    if (runs == 0 || runs * 4 > n_kmers) return 0;
-    SBWT_TRY(grow(w.kstart, w.kstart_cap, runs + 1));
-    SBWT_TRY(grow(w.rows, w.rows_cap, runs + 1));
-    SBWT_TRY(grow(w.chunk_row, w.chunk_cap, (n_kmers + chunk - 1) / chunk));
-    run_table_kernel<<<(unsigned)nb, kWords, 0, s>>>(positions, n_kmers, bits, counts, runs, chunk / 32u, w.kstart,
-                                                     w.rows, w.chunk_row);
+    run_table_kernel<<<(unsigned)nb, kWords, 0, s>>>(positions, n_kmers, bits, counts, counts + nb, chunk / 32u,
+                                                     w.kstart, w.rows, w.chunk_row);
     SBWT_CHECK_CUDA(cudaGetLastError());
-    *n_rows = runs;
+    *runs_dev = counts + nb;
     return 0;
 }
 

@@ -49,6 +49,7 @@ template <int KPT> struct MinBlocks { static constexpr int value = KPT <= 1 ? 4 
 
 template <class R, int KPT, int TPK>
 __global__ void __launch_bounds__(256, MinBlocks<KPT>::value) search_kernel(const R rk, const SearchArgs a) {
+    if (a.runs_dev && runs_usable(*a.runs_dev, a.n_kmers)) return;  // the run walk takes this kernel-contract call
     using IT = typename R::IT;
     using PT = typename PairOf<IT>::T;
     const u32 lane = threadIdx.x & 31u;
@@ -197,6 +198,7 @@ struct QEntry {
 
 template <class R>
 __global__ void __launch_bounds__(128) search_queue_kernel(const R rk, const SearchArgs a) {
+    if (a.runs_dev && runs_usable(*a.runs_dev, a.n_kmers)) return;  // the run walk takes this kernel-contract call
     static_assert(sizeof(typename R::IT) == 4, "the queue form serves 32-bit intervals");
     __shared__ QEntry queue[kQueueWarps][kQueue];
     using PT = uint2;
@@ -485,6 +487,9 @@ struct RunEntry {
 // batch's letters, k-mers and rows stay below 2^32 - 2^16, run32_ok; else u64).
 template <class R, bool STREAM, bool FILTER, u32 WIN, class IX>
 __global__ void __launch_bounds__(128, RunsMinBlocks<R, IX>::value) search_runs_kernel(const R rk, const SearchArgs a) {
+    // kernel contract: the run count is on the device; too few runs and the per-k-mer search takes the call
+    const u64 n_rows = a.runs_dev ? *a.runs_dev : a.n_rows;
+    if (a.runs_dev && !runs_usable(n_rows, a.n_kmers)) return;
     static_assert(sizeof(typename R::IT) == 4, "the run form serves 32-bit intervals");
     static_assert(WIN % 32 == 0, "windows cover whole bitmap words");
     __shared__ RunEntry queue[kQueueWarps][kQueue];
@@ -503,7 +508,7 @@ __global__ void __launch_bounds__(128, RunsMinBlocks<R, IX>::value) search_runs_
     __syncthreads();
     const u32 rootR = (u32)(a.C[4] - 1ull);
     const PT *pre = reinterpret_cast<const PT *>(a.pre);
-    const IX n_eff = (IX)min(a.n_kmers, a.kstart[a.n_rows]);
+    const IX n_eff = (IX)min(a.n_kmers, a.kstart[n_rows]);
     uint32_t *const member = a.member;
     RunEntry *q = queue[warp];
 #if SBWT_ANSWER_WRITE_ONCE

@@ -645,6 +645,29 @@ def test_build_times_reported(small, cuda):
         assert ix.build_times()["presearch_ms"] > 0
 
 
+def test_search_packed_back_to_back_calls_without_a_wait(small, cuda):
+    """The kernel contract chooses between the run walk and the per-k-mer search on the device: calls
+    on runs, shuffled positions and runs again, issued back to back with no synchronisation between
+    them, each answer as the oracle does."""
+    import torch
+    b, k = small["built"], small["k"]
+    ox = orc.OracleIndex(b.bits, b.n_bits)
+    words = orc.pack(small["letters"])
+    runs = orc.positions(small["rows"], k).copy()
+    shuffled = runs[np.random.default_rng(5).permutation(runs.size)]
+    want_runs, want_shuf = ox.search_positions(words, runs, k, 10), ox.search_positions(words, shuffled, k, 10)
+    with sg.Index.from_bits(b.bits, b.n_bits, k=k, k_presearch=10) as ix:
+        d_words = _t(words, cuda)
+        d = [_t(x, cuda) for x in (runs, shuffled, runs, shuffled[: shuffled.size // 2])]
+        torch.cuda.synchronize()
+        for x in d:
+            ix.search_packed(d_words, x)
+        torch.cuda.synchronize()
+    assert np.array_equal(_u64(d[0]), want_runs) and np.array_equal(_u64(d[2]), want_runs)
+    assert np.array_equal(_u64(d[1]), want_shuf)
+    assert np.array_equal(_u64(d[3]), want_shuf[: shuffled.size // 2])
+
+
 @pytest.mark.parametrize("mode", [0, 1, 2])
 @pytest.mark.parametrize("order", ["reads", "shuffled", "mixed"])
 def test_search_packed_runs_and_random_positions(small, cuda, mode, order):
