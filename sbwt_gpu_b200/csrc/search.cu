@@ -196,8 +196,15 @@ struct QEntry {
     u32 l, r;
 };
 
+// Resident blocks per SM the line ranker's queue kernel is compiled for: with C
+// read from shared memory it fits 10 (48 registers, no spill).  Measured on the
+// large workload, every k-mer searched: 40.1 ms against 42.5 at the compiler's 9
+// blocks; 12 blocks (40 registers, 48 bytes of spill) 44.2.
+template <class R> struct QueueMinBlocks { static constexpr int value = 1; };
+template <int TPK> struct QueueMinBlocks<LinesRankerT<TPK>> { static constexpr int value = 10; };
+
 template <class R>
-__global__ void __launch_bounds__(128) search_queue_kernel(const R rk, const SearchArgs a) {
+__global__ void __launch_bounds__(128, QueueMinBlocks<R>::value) search_queue_kernel(const R rk, const SearchArgs a) {
     if (a.runs_dev && runs_usable(*a.runs_dev, a.n_kmers)) return;  // the run walk takes this kernel-contract call
     static_assert(sizeof(typename R::IT) == 4, "the queue form serves 32-bit intervals");
     __shared__ QEntry queue[kQueueWarps][kQueue];
@@ -205,7 +212,9 @@ __global__ void __launch_bounds__(128) search_queue_kernel(const R rk, const Sea
     const u32 lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const u32 lt = (1u << lane) - 1u;
     const u32 k = a.k, p = a.p;
-    const u32 C0 = (u32)a.C[0], C1 = (u32)a.C[1], C2 = (u32)a.C[2], C3 = (u32)a.C[3];
+    __shared__ u32 sC[4];  // C in shared memory: registers kept for the search state
+    if (threadIdx.x < 4) sC[threadIdx.x] = (u32)a.C[threadIdx.x];
+    __syncthreads();
     const u32 rootR = (u32)(a.C[4] - 1ull);
     const PT *pre = reinterpret_cast<const PT *>(a.pre);
     const bool read_mode = !a.positions && !a.kmer_list;
@@ -319,7 +328,7 @@ __global__ void __launch_bounds__(128) search_queue_kernel(const R rk, const Sea
         if (I != kDone) {
             const u32 c = (u32)((kmer >> (62u - 2u * I)) & 3u);
             const typename R::Fetch f = rk.fetch(c, L, Rr, 0);
-            const u32 Cc = c == 0 ? C0 : c == 1 ? C1 : c == 2 ? C2 : C3;
+            const u32 Cc = sC[c];
             rk.finish(f, Cc, L, Rr, 0, kFull);
             I++;
             if (L > Rr || I >= k) {
