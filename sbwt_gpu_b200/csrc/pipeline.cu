@@ -232,6 +232,50 @@ bool host_has_avx2() {
     static const bool yes = __builtin_cpu_supports("avx2");
     return yes;
 }
+
+// The same with AVX-512: blocks of 8 answers, one 64-byte (whole cache line)
+// streaming store each, built without branches: the found node ids of the
+// block are expand-loaded into the lanes of its set membership bits, widened
+// to 64 bits and blended with ~0 for the absent k-mers.
+__attribute__((target("avx512f,avx512vl"))) void expand_groups_avx512(u64 *answers, u64 nk, const uint32_t *member,
+                                                                      const u64 *goff, const uint32_t *nodes, u64 g0,
+                                                                      u64 g1) {
+    const u64 j0 = g0 * kGroupWords * 32u, j1 = std::min<u64>(g1 * kGroupWords * 32u, nk);
+    if (j0 >= j1) return;
+    u64 o = goff[g0];
+    auto bit = [&](u64 j) { return (member[j >> 5] >> (j & 31u)) & 1u; };
+    u64 j = j0;
+    // head: up to the first 64-byte boundary of the output
+    while (j < j1 && (reinterpret_cast<uintptr_t>(answers + j) & 63u)) {
+        const u32 b = bit(j);
+        store_stream(answers + j, b ? (u64)nodes[o] : ~0ull);
+        o += b;
+        j++;
+    }
+    const __m512i none = _mm512_set1_epi64(-1);
+    for (; j + 8 <= j1; j += 8) {
+        // the 8 bits of k-mers j .. j+7 (they may straddle two bitmap words, both below nk)
+        const u64 w = j >> 5;
+        const u32 sh = (u32)(j & 31u);
+        const u64 pair = (u64)member[w] | (sh > 24u ? (u64)member[w + 1] << 32 : 0ull);
+        const __mmask8 m8 = (__mmask8)((pair >> sh) & 0xffu);
+        const __m256i n32 = _mm256_maskz_expandloadu_epi32(m8, nodes + o);  // reads popcount(m8) ids
+        const __m512i v = _mm512_mask_blend_epi64(m8, none, _mm512_cvtepu32_epi64(n32));
+        _mm512_stream_si512(reinterpret_cast<__m512i *>(answers + j), v);
+        o += (u64)__builtin_popcount((unsigned)m8);
+    }
+    for (; j < j1; j++) {  // tail
+        const u32 b = bit(j);
+        store_stream(answers + j, b ? (u64)nodes[o] : ~0ull);
+        o += b;
+    }
+}
+
+bool host_has_avx512() {
+    static const bool yes = __builtin_cpu_supports("avx512f") && __builtin_cpu_supports("avx512vl");
+    if (const char *e = std::getenv("SBWT_EXPAND_AVX512")) return yes && e[0] != '0';
+    return yes;
+}
 #endif
 
 // answers[j] for the nk k-mers of one chunk from its sparse form (streaming
@@ -247,7 +291,10 @@ void expand_answers(u64 *answers, u64 nk, const uint32_t *member, const u64 *gof
             // contiguous runs of groups per thread: contiguous output, aligned blocks inside
             const u64 nt = (u64)omp_get_num_threads(), t = (u64)omp_get_thread_num();
             const u64 per = (ng + nt - 1) / nt;
-            expand_groups_avx2(answers, nk, member, goff, nodes, std::min(ng, t * per), std::min(ng, (t + 1) * per));
+            if (host_has_avx512())
+                expand_groups_avx512(answers, nk, member, goff, nodes, std::min(ng, t * per), std::min(ng, (t + 1) * per));
+            else
+                expand_groups_avx2(answers, nk, member, goff, nodes, std::min(ng, t * per), std::min(ng, (t + 1) * per));
             store_fence();
         }
         return;
