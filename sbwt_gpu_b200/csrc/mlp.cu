@@ -563,11 +563,13 @@ __global__ void enumerate_kernel(const ulonglong4 *lines, u32 lpc, C5 C5v, u32 n
     out[v - 1] = node_kmer(lines, lpc, C, k, v, x) ? x : ~0ull;
 }
 
+// labels[i] = answers[i] found (labels == NULL: only count them, for lists
+// longer than any label array).
 __global__ void labels_kernel(const u64 *__restrict__ answers, u64 n, uint8_t *__restrict__ labels,
                               unsigned long long *positives) {
     const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     const bool hit = i < n && answers[i] != ~0ull;
-    if (i < n) labels[i] = hit ? 1 : 0;
+    if (labels && i < n) labels[i] = hit ? 1 : 0;
     const u32 m = __ballot_sync(0xffffffffu, hit);
     if ((threadIdx.x & 31u) == 0 && m) atomicAdd(positives, (unsigned long long)__popc(m));
 }

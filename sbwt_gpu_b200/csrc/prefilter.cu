@@ -393,11 +393,12 @@ extern "C" int sbwt_prefilter_train(sbwt_index *ix, const sbwt_mlp_params *prm, 
         if (rc) break;
         rc = check_err(pf->d_err, "prefilter inference");
         if (rc) break;
-        // indexed k-mers = nodes that are not dummies
+        // indexed k-mers = nodes that are not dummies (counted only: d_labels holds the n_train
+        // training labels, fewer than the nodes of a large index)
         {
             unsigned long long *cnt = d_cnt;
             cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s);
-            labels_kernel<<<(unsigned)((nodes + 255) / 256), 256, 0, s>>>(d_all, nodes, d_labels, cnt);
+            labels_kernel<<<(unsigned)((nodes + 255) / 256), 256, 0, s>>>(d_all, nodes, nullptr, cnt);
             unsigned long long c = 0;
             cudaMemcpyAsync(&c, cnt, sizeof(c), cudaMemcpyDeviceToHost, s);
             cudaStreamSynchronize(s);

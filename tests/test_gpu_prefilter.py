@@ -236,3 +236,23 @@ def test_filtered_reads_pangenome_shape(cuda):
         with sg.Prefilter.train(ix, steps=300, batch=2048, n_positive=300_000, n_negative=300_000, seed=3) as pf:
             skipped, nk, want = _filtered_vs_oracle(ix, pf, built, letters, rows, k, 12, cuda)
     assert 0 < skipped < nk
+
+
+def test_sandwich_holds_when_the_index_has_more_kmers_than_the_training_set(cuda):
+    """The backup Bloom filter covers every indexed k-mer the model rejects, also when the index has more
+    k-mers than the training set has samples (the count of indexed k-mers must not use the training
+    labels' buffer).  With tau far above any logit the model rejects every k-mer, so the filter must
+    hold all of them and the answers must still equal the oracle's."""
+    rng = wl.rng_for(57)
+    k = 31
+    genome = wl.random_bases(rng, 300_000)
+    built = sg.build_sbwt([genome.tobytes()], k)
+    letters, rows = wl.mixed_reads(rng, genome, 400, 400, 150, 0.01)
+    with sg.Index.from_bits(built.bits, built.n_bits, k=k, k_presearch=10) as ix:
+        with sg.Prefilter.train(ix, steps=5, batch=2048, n_positive=4096, n_negative=4096, seed=5,
+                                tau=1e9) as pf:
+            st = pf.stats()
+            assert st["n_train"] == 8192 < built.n_bits // 10
+            assert st["n_rejected_indexed"] == st["n_indexed_kmers"] > 250_000
+            skipped, nk, want = _filtered_vs_oracle(ix, pf, built, letters, rows, k, 10, cuda)
+    assert (want != orc.NOT_FOUND).any() and 0 < skipped < nk
